@@ -1,0 +1,337 @@
+"""Benchmark: primaries/s of the plain wavefront transport on one B200.
+
+Workload (one step): the line-space grating scan -- 8 PMMA-like trapezoidal
+lines (pitch 32 nm, top CD 16 nm, 86 deg sidewalls, 30 nm high, 4 144
+triangles) on a Si-like substrate; 256 x 256 pixels at 0.5 nm x 100 primaries
+per pixel = 6 553 600 primaries at 500 eV with a 1 nm Gaussian spot;
+detector plane at z = 50 nm.  Synthetic geometry, materials and primaries of
+those shapes (no external data).  A step is the whole scan: every primary
+and its full secondary cascade.
+
+value: primaries/s with the primary records already in HBM when the timed
+       region starts (a device-to-device push, then the run).
+e2e:   the same through the public API from pinned host records: host->device
+       copy of the primaries, the run, device->host copy of every detected
+       36-byte record and of the tallies, all inside the timed region.
+
+Multi-GPU (torchrun): replicas, one scan per rank with its own seed (weak
+scaling); time = max over ranks.  --impl reference times the reference's own
+multithreaded CPU driver (oracle/_ref/nebula_cpu_mt built from its sources)
+on a bounded sample of the same scan with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "primaries/s on 1 B200, plain vs batched; adjoint:forward time at yield err ≤3σ"
+BYTES_PER_EVENT = 96   # 48-byte electron state read + written per event
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_inputs(workdir, seed):
+    from nebula_b200.synth import workloads, geometry, materials, nmat
+    w = workloads.grating(seed=seed)
+    tri = os.path.join(workdir, "grating.tri")
+    geometry.write_tri(tri, w.triangles)
+    mats = []
+    for spec in w.material_specs:
+        p = os.path.join(workdir, spec.name + ".nmat")
+        nmat.write(p, materials.build_raw_material(spec))
+        mats.append(p)
+    return w, tri, mats
+
+
+# ---------------------------------------------------------------------------- CPU
+def run_reference_cpu(tri, mats, pri_records, workdir):
+    """The reference's own multithreaded CPU driver on the given primaries.
+    Returns (primaries/s from its 'Simulation' timer, seconds, wall seconds)."""
+    from nebula_b200.synth import primaries
+    from oracle import oracle as O
+    pri_path = os.path.join(workdir, "sample.pri")
+    primaries.write_pri(pri_path, pri_records)
+    t0 = time.time()
+    r = subprocess.run([O.REF_CPU_MT, tri, pri_path] + mats, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                       text=True)
+    wall = time.time() - t0
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    m = re.search(r"Simulation:\s*([0-9.]+)", r.stderr)
+    sim_s = float(m.group(1)) if m else wall
+    return len(pri_records) / sim_s, sim_s, wall
+
+
+def cpu_sample(w, cores, per_core):
+    """A bounded, contiguous block of pixels of the scan (rows from the top)."""
+    n_pix = max(1, int(cores * per_core) // 100)
+    return w.primaries[: n_pix * 100], n_pix
+
+
+def cpu_baseline(w, tri, mats, workdir):
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    sample, n_pix = cpu_sample(w, cores, 20000)
+    if os.path.exists(O.REF_CPU_MT):
+        rate, sim_s, wall = run_reference_cpu(tri, mats, sample, workdir)
+        return {"value": rate, "unit": "primaries/s", "cores": cores, "kind": "reference",
+                "sample": "%d pixels x 100 primaries (%d) of the scan, reference nebula_cpu_mt, %d threads, "
+                          "its Simulation timer %.2f s" % (n_pix, len(sample), cores, sim_s)}
+    # the oracle port when the reference build is absent
+    import nebula_b200 as nb  # noqa: F401
+    om = [O.Material(p) for p in mats]
+    g = nb.Geometry.from_tri_file(tri)
+    od, tr = g.export()
+    inf = g.info()
+    t11 = np.concatenate([np.stack([tr["material_in"], tr["material_out"]], 1).astype(np.float32),
+                          tr["r0"], tr["e1"], tr["e2"]], 1)
+    og = O.Geometry(od, t11, inf["center"], inf["halfsize"], inf["max_extent"])
+    t0 = time.time()
+    O.simulate(og, om, sample, 1, threads=cores)
+    dt = time.time() - t0
+    return {"value": len(sample) / dt, "unit": "primaries/s", "cores": cores, "kind": "port",
+            "sample": "%d primaries of the scan, oracle restatement, %d threads" % (len(sample), cores)}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not os.path.exists(O.REF_CPU_MT):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref/nebula_cpu_mt missing"}))
+        return
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        w, tri, mats = make_inputs(d, seed=7)
+        sample, n_pix = cpu_sample(w, cores, 10000)
+        for _ in range(args.warmup):
+            run_reference_cpu(tri, mats, sample[: max(100, len(sample) // 10)], d)
+        rates, secs = [], []
+        for _ in range(args.steps):
+            r, s, _ = run_reference_cpu(tri, mats, sample, d)
+            rates.append(r)
+            secs.append(s)
+    value = len(sample) * len(secs) / sum(secs)
+    desc = "%d pixels x 100 primaries (%d) of the scan per step, reference nebula_cpu_mt, %d threads" % (
+        n_pix, len(sample), cores)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "primaries/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(secs)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "grating-256x256x100-500eV (bounded CPU sample)", "sample": desc},
+        "cpu_baseline": {"value": value, "unit": "primaries/s", "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ---------------------------------------------------------------------------- GPU
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--capacity", type=int, default=1 << 21)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import nebula_b200 as nb
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = local
+
+    with tempfile.TemporaryDirectory() as d:
+        w, tri, mats = make_inputs(d, seed=7)
+        g = nb.Geometry.from_tri_file(tri)
+        ms = [nb.Material.load(p) for p in mats]
+        n_pri = len(w.primaries)
+        stream = torch.cuda.Stream(device=dev)
+        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=1000 + rank, device=dev, tally=w.n_pixels,
+                            stream=stream.cuda_stream)
+        pri_dev = torch.from_numpy(w.primaries.view(np.uint8)).to(f"cuda:{dev}")
+        pri_host = torch.from_numpy(w.primaries.view(np.uint8).copy()).pin_memory()
+
+        def step_device():
+            sim.reset()
+            sim.push_device(pri_dev.data_ptr(), n_pri)
+            sim.run()
+
+        def step_e2e():
+            sim.reset()
+            sim.push(np.frombuffer(pri_host.numpy(), dtype=nb.PRI_DTYPE))
+            sim.run()
+            rec = sim.flush_detected()
+            tal = sim.tallies()
+            return rec, tal
+
+        for _ in range(args.warmup):
+            step_device()
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+
+        # timed: device-resident inputs
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        kernel_ms = 0.0
+        flights = 0
+        iters = 0
+        detected = 0
+        with ClockSampler(dev) as clk:
+            torch.cuda.synchronize(dev)
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step_device()
+                c = sim.counters()
+                kernel_ms += sim.kernel_ms()
+                flights += c["flights"]
+                iters += c["iterations"]
+                detected += c["detected"]
+            ev1.record(stream)
+            torch.cuda.synchronize(dev)
+        ms = ev0.elapsed_time(ev1)
+        if dist:
+            t = torch.tensor([ms], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+
+        # timed: end to end from pinned host records
+        h2d = n_pri * 36
+        d2h = 0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            rec, tal = step_e2e()
+            d2h = len(rec) * 36 + sum(x.nbytes for x in tal if x is not None)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([e2e_ms], device=f"cuda:{dev}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        sim.close()
+
+        value = n_pri * args.steps * world / (ms / 1000.0)
+        e2e_value = n_pri * args.steps * world / (e2e_ms / 1000.0)
+        peak, peak_kind = measured_peaks()
+        achieved = flights * BYTES_PER_EVENT / (kernel_ms / 1000.0) / 1e9
+        out = {
+            "metric": METRIC, "value": value, "unit": "primaries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "grating-256x256x100-500eV", "method": "plain wavefront",
+                       "primaries_per_step": n_pri, "triangles": int(len(w.triangles)),
+                       "capacity": args.capacity, "parallelism": "replicas x%d" % world,
+                       "l2": "inputs larger than L2 (primaries 236 MB, queues > 1 GB)"},
+            "events_per_primary": flights / (n_pri * args.steps),
+            "detected_per_primary": detected / (n_pri * args.steps),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "%d B algorithmic per event x %d events / transport-kernel time %.1f ms; "
+                                 "peak %s" % (BYTES_PER_EVENT, flights, kernel_ms, peak_kind)},
+            "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": iters,
+            "clocks": clk.summary(),
+        }
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            try:
+                out["cpu_baseline"] = cpu_baseline(w, tri, mats, d)
+            except Exception as e:  # reported, not fatal
+                out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        if rank == 0:
+            print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,252 @@
+/*
+ * nebula_b200 -- C ABI of the B200 electron-transport library.
+ *
+ * Plain C types only: every entry point returns an nbl_status, never throws,
+ * and copies caller arrays during the call (the library owns all device
+ * memory; the caller owns host arrays).  A simulation handle is bound to one
+ * device and one CUDA stream; calls on one handle are not thread-safe,
+ * distinct handles are independent.
+ *
+ * Reference interfaces each group replaces (paths relative to the
+ * reference's source/ directory):
+ *   materials   material<scatter_list<full_penn, kieft_elastic>>(hdf5_file)
+ *               core/material.inl:13-18, physics/full_penn.h:294-406,
+ *               physics/kieft/elastic.h:120-166
+ *   geometry    nbl::load_tri_file io/load_tri_file.cpp:8-60;
+ *               octree_builder::octree_root + linearized_octree
+ *               geometry/octree/octree_builder.cpp:171-352;
+ *               octree<true>::create geometry/octree.inl:3-7, 279-313
+ *   ray query   octree<gpu_flag>::propagate geometry/octree.inl:33-192
+ *   simulation  gpu_driver<scatter_physics, intersect_t, octree>
+ *               drivers/gpu/gpu_driver.h:56-178 (constructor, push,
+ *               push_to_simulation, do_iteration, buffer_detected,
+ *               flush_buffered, get_running_count, get_detected_count)
+ *   records     36-byte primary / detected records io/load_pri_file.cpp:112-121,
+ *               gpu_main.cu:216-223
+ *   physics     compile-time physics selection physics_config.h:20-46
+ */
+#ifndef NEBULA_B200_H
+#define NEBULA_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NBL_ABI_VERSION 1
+
+typedef enum nbl_status {
+	NBL_OK = 0,
+	NBL_ERR_INVALID_ARG = 1,
+	NBL_ERR_OOM = 2,
+	NBL_ERR_CUDA = 3,
+	NBL_ERR_BUDGET_EXCEEDED = 4,   /* iteration / event budget ran out */
+	NBL_ERR_NAN_STATE = 5,         /* an electron reached a NaN state */
+	NBL_ERR_POOL_OVERFLOW = 6,     /* an event queue or the record buffer overflowed */
+	NBL_ERR_IO = 7,                /* file missing or malformed */
+	NBL_ERR_NO_DEVICE = 8
+} nbl_status;
+
+/* Message of the last failing call on this thread (never NULL). */
+const char* nbl_last_error_string(void);
+int nbl_abi_version(void);
+
+/* Special material ids (core/material_manager.h:77-86). */
+#define NBL_MAT_NOP (-128)
+#define NBL_MAT_TERMINATOR (-127)
+#define NBL_MAT_DETECTOR (-126)
+#define NBL_MAT_DETECTOR_LT50 (-125)
+#define NBL_MAT_DETECTOR_GE50 (-124)
+#define NBL_MAT_VACUUM (-123)
+#define NBL_MAT_MIRROR (-122)
+
+/* ------------------------------------------------------------ records */
+/* Primary electron / detected electron, 36 bytes little-endian:
+ * position (nm), direction (unnormalised), kinetic energy (eV), pixel. */
+typedef struct nbl_record {
+	float pos[3];
+	float dir[3];
+	float energy;
+	int32_t px, py;
+} nbl_record;
+
+/* Triangle, the reference member layout (core/triangle.h:66-76): the normal
+ * (r1-r0)x(r2-r0) points from material_in to material_out; e1 = r1-r0 and
+ * e2 = r2-r0 are computed in float. */
+typedef struct nbl_triangle {
+	int32_t material_in;
+	int32_t material_out;
+	float r0[3];
+	float e1[3];
+	float e2[3];
+} nbl_triangle;
+
+/* Read a .tri file (11 columns: in out x0 y0 z0 x1 y1 z1 x2 y2 z2, nm).
+ * *out is allocated by the library; release with nbl_free. */
+nbl_status nbl_load_tri_file(const char* path, nbl_triangle** out, int64_t* n);
+/* Read a .pri file of 36-byte records; release with nbl_free. */
+nbl_status nbl_load_pri_file(const char* path, nbl_record** out, int64_t* n);
+void nbl_free(void* p);
+
+/* ------------------------------------------------------------ materials */
+/* A table in the reference's transformed domain (common/util/table_{1,2,3}D):
+ * dense row-major data[nx][ny][nz] (ny = nz = 1 for 1-D, nz = 1 for 2-D),
+ * index along each axis = (value - min) * step. */
+typedef struct nbl_table {
+	int32_t nx, ny, nz;
+	float x_min, x_step, y_min, y_step, z_min, z_step;
+	const float* data;
+} nbl_table;
+
+/* Tables and constants of one material after full_penn::create and
+ * kieft_elastic::create:
+ *   el_imfp   log(elastic 1/lambda / nm^-1)      over log(E/eV)
+ *   el_icdf   cos(theta)                          over log(E/eV) x P
+ *   in_imfp   log(inelastic 1/lambda / nm^-1)    over log(E/eV)
+ *   in_omega  log(omega/eV)                       over log(E/eV) x P
+ *   in_q      hbar q / sqrt(2m) in eV^1/2         over log(E/eV) x omega/E x P
+ *   in_binding binding energy in eV, -1 = none    over log(E/eV) x log(omega/E) x P
+ * barrier = fermi + work function (eV); band_gap -1 for metals;
+ * recoil_const = 4 m_e / M (elastic.h:161-163). */
+typedef struct nbl_material_tables {
+	nbl_table el_imfp, el_icdf, in_imfp, in_omega, in_q, in_binding;
+	float fermi, band_gap, barrier, phonon_loss, recoil_const;
+} nbl_material_tables;
+
+typedef struct nbl_material nbl_material;
+
+/* Load a material file (.nmat: the self-describing binary equivalent of the
+ * reference's HDF5 material file) and apply the reference's table transforms. */
+nbl_status nbl_material_load(const char* path, nbl_material** out);
+/* Create from tables already in the transformed domain (copied). */
+nbl_status nbl_material_create(const nbl_material_tables* tables, nbl_material** out);
+/* Views of the material's tables (valid while the material lives). */
+nbl_status nbl_material_get_tables(const nbl_material* m, nbl_material_tables* out);
+/* Largest energy all tables cover (scatter_list::get_max_energy). */
+nbl_status nbl_material_max_energy(const nbl_material* m, float* out);
+void nbl_material_destroy(nbl_material* m);
+
+/* ------------------------------------------------------------ geometry */
+typedef struct nbl_geometry nbl_geometry;
+
+/* Build the octree from triangles the way octree_builder does: cells split
+ * above `split_count` triangles until `max_depth` (reference: 16 and 21;
+ * pass 0 for those defaults), triangle-box overlap on 1.01x inflated cells,
+ * root box = triangle bounds + 1 nm, breadth-first linearisation with
+ * triangles in first-leaf order. */
+nbl_status nbl_geometry_build(const nbl_triangle* tris, int64_t n, int32_t max_depth, int32_t split_count,
+	nbl_geometry** out);
+/* Use an already linearised octree (octree_builder.h:209-248 layout). */
+nbl_status nbl_geometry_from_linearized(const int32_t* octree_data, int64_t n_octree,
+	const nbl_triangle* tris, int64_t n_tri, const float center[3], const float halfsize[3],
+	nbl_geometry** out);
+/* Sizes and domain of a geometry. */
+nbl_status nbl_geometry_info(const nbl_geometry* g, int64_t* n_octree, int64_t* n_tri,
+	float center[3], float halfsize[3], float* max_extent);
+/* Copy out the linearised octree and its triangle order. */
+nbl_status nbl_geometry_export(const nbl_geometry* g, int32_t* octree_data, nbl_triangle* tris);
+void nbl_geometry_destroy(nbl_geometry* g);
+
+/* Device batch of octree walks on host arrays (n rays): nearest triangle hit
+ * within dist[i] along the normalised dir, ignoring triangle ignore_tri[i]
+ * (-1: none) and triangles whose outgoing material is ignore_mat[i].
+ * Results equal octree<false>::propagate bit for bit: out_dist is dist[i]
+ * and out_tri -1 when nothing is hit. */
+nbl_status nbl_ray_query(const nbl_geometry* g, int device, int64_t n, const float* pos, const float* dir,
+	const float* dist, const int32_t* ignore_tri, const int32_t* ignore_mat, float* out_dist, int32_t* out_tri);
+
+/* ------------------------------------------------------------ physics */
+/* Physics options, mirroring physics_config.h:20-46.  The build compiles the
+ * reference's default selection; other values are rejected. */
+typedef struct nbl_physics_opts {
+	int32_t inelastic_model;        /* 0: Full Penn (the only one built) */
+	int32_t generate_secondaries;   /* 1 */
+	int32_t acoustic_phonon_loss;   /* 1 */
+	int32_t atomic_recoil_loss;     /* 1 */
+	int32_t quantum_transmission;   /* 1 */
+	int32_t interface_refraction;   /* 1 */
+	int32_t interface_absorption;   /* 0 */
+} nbl_physics_opts;
+void nbl_physics_defaults(nbl_physics_opts* o);
+
+/* ------------------------------------------------------------ simulation */
+typedef struct nbl_params {
+	int32_t device;              /* CUDA device ordinal */
+	uint32_t capacity;           /* electrons in flight (refill target); 0: 1 << 20 */
+	float energy_threshold;      /* eV above the vacuum level, gpu_driver.h:56-59 */
+	uint64_t seed;
+	uint32_t block_size;         /* 0: 256 */
+	uint32_t grid_size;          /* 0: all SMs at full occupancy */
+	uint32_t iterations_per_graph; /* 0: 24 (multiple of 3) */
+	uint32_t record_capacity;    /* detected records buffered on the device; 0: max(4 * capacity, 2^20) */
+	int32_t tally_nx, tally_ny;  /* per-pixel SE / BSE tallies over px in [0,nx), py in [0,ny); 0: off */
+	int32_t hist_bins;           /* detected-energy histogram; 0: 200 */
+	float hist_emax;             /* eV; 0: 1000 */
+	uint32_t max_events;         /* per-electron flight budget; 0: 1 << 22 */
+	void* stream;                /* cudaStream_t to run on; NULL: a library-owned stream */
+	nbl_physics_opts physics;
+	int32_t adjoint;             /* 1: accumulate score functions (see nbl_adjoint_*) */
+} nbl_params;
+void nbl_params_defaults(nbl_params* p);
+
+typedef struct nbl_sim nbl_sim;
+
+typedef struct nbl_counters {
+	uint64_t flights;            /* free flights = driver iterations of the reference */
+	uint64_t boundary, elastic, inelastic;
+	uint64_t spawned, detected, terminated, primaries_started;
+	uint64_t walk_overflow, nan_state, queue_overflow, record_overflow, event_budget;
+	uint64_t deferred;           /* inelastic events postponed for lack of secondary room */
+	uint64_t iterations;         /* wavefront iterations launched */
+	uint64_t primaries_total;    /* primaries pushed */
+	uint64_t records_pending;    /* detected records not yet drained */
+} nbl_counters;
+
+nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
+	const nbl_params* params, nbl_sim** out);
+/* Queue primaries (host records; tag = running index; pixel kept for the
+ * detected records).  Mirrors gpu_driver::push / push_to_buffer. */
+nbl_status nbl_sim_push_primaries(nbl_sim* s, const nbl_record* recs, int64_t n);
+/* Same from device memory (records already resident in HBM). */
+nbl_status nbl_sim_push_primaries_device(nbl_sim* s, const void* d_recs, int64_t n);
+/* Run `iterations` wavefront iterations (rounded up to whole graphs); the
+ * number still in flight or queued is returned (gpu_driver::do_iteration,
+ * get_running_count). */
+nbl_status nbl_sim_step(nbl_sim* s, uint32_t iterations, int64_t* running);
+/* Run until every queued primary and its cascade is done. */
+nbl_status nbl_sim_run(nbl_sim* s);
+/* Copy detected records out (flush_buffered); *n gets the number written. */
+nbl_status nbl_sim_drain_detected(nbl_sim* s, nbl_record* out, int64_t cap, int64_t* n);
+/* Pending detected records on the device. */
+nbl_status nbl_sim_detected_count(nbl_sim* s, int64_t* n);
+/* Tallies: se/bse per pixel (tally_nx * tally_ny each, may be NULL),
+ * histogram (hist_bins, may be NULL). */
+nbl_status nbl_sim_tallies(nbl_sim* s, uint32_t* se_img, uint32_t* bse_img, uint32_t* hist);
+nbl_status nbl_sim_counters(nbl_sim* s, nbl_counters* out);
+/* Clear tallies, counters and records, forget pushed primaries, keep geometry
+ * and materials (a new scan on the same sample). */
+nbl_status nbl_sim_reset(nbl_sim* s);
+/* Device time of the transport iterations run so far (CUDA events around
+ * each graph launch), milliseconds. */
+nbl_status nbl_sim_kernel_ms(nbl_sim* s, double* ms);
+void nbl_sim_destroy(nbl_sim* s);
+
+/* ------------------------------------------------------------ debug entry points */
+/* Table lookups on the device (which: 0 el_imfp 1 el_icdf 2 in_imfp 3 in_omega
+ * 4 in_q 5 in_binding) for n points; `rounddown` selects get_rounddown. */
+nbl_status nbl_debug_table_lookup(const nbl_material* m, int device, int32_t which, int32_t rounddown,
+	int64_t n, const float* x, const float* y, const float* z, float* out);
+/* One event per case on the device with caller-supplied uniforms (n_uniforms
+ * per case).  kind 1 inelastic, 2 elastic, 3 boundary crossing of triangle
+ * tri[i] (geometry g).  state: 7 floats (pos, dir, E) in, out. */
+nbl_status nbl_debug_event(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
+	int device, int32_t kind, int64_t n, const float* state_in, const int32_t* mat_in, const int32_t* tri,
+	const float* uniforms, int32_t n_uniforms, float* state_out, int32_t* mat_out, int32_t* status,
+	float* se_out, int32_t* has_se, int32_t* used);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,963 @@
+// C ABI: geometry, materials, device uploads, the wavefront run loop and the
+// debug entry points.  See include/nebula_b200.h for the contract.
+#include "internal.hpp"
+#include "../kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstring>
+#include <cstdio>
+#include <fstream>
+#include <sstream>
+#include <algorithm>
+#include <memory>
+
+using namespace nbl;
+
+namespace nbl {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& m) { g_last_error = m; }
+
+#define CU(call)                                                                          \
+	do {                                                                                  \
+		cudaError_t e_ = (call);                                                          \
+		if (e_ != cudaSuccess)                                                            \
+			throw Error(e_ == cudaErrorMemoryAllocation ? NBL_ERR_OOM : NBL_ERR_CUDA,     \
+				std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+	} while (0)
+
+namespace {
+
+void set_device(int device)
+{
+	int n = 0;
+	if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+		throw Error(NBL_ERR_NO_DEVICE, "no CUDA device available");
+	require(device >= 0 && device < n, "device ordinal out of range");
+	CU(cudaSetDevice(device));
+}
+
+// Device buffer that frees itself.
+struct DevBuf {
+	void* p = nullptr;
+	size_t bytes = 0;
+	DevBuf() = default;
+	explicit DevBuf(size_t n) { alloc(n); }
+	void alloc(size_t n)
+	{
+		release();
+		if (n == 0) return;
+		CU(cudaMalloc(&p, n));
+		bytes = n;
+	}
+	void release()
+	{
+		if (p) cudaFree(p);
+		p = nullptr;
+		bytes = 0;
+	}
+	~DevBuf() { release(); }
+	DevBuf(const DevBuf&) = delete;
+	DevBuf& operator=(const DevBuf&) = delete;
+	template<class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Triangles in the 64-byte device layout; normal = cross(e1, e2) in float
+// with the operations of triangle::get_normal (core/triangle.inl:75-78).
+std::vector<DevTriangle> device_triangles(const std::vector<nbl_triangle>& tris)
+{
+	std::vector<DevTriangle> out(tris.size());
+	for (size_t i = 0; i < tris.size(); ++i) {
+		const nbl_triangle& t = tris[i];
+		DevTriangle& d = out[i];
+		d.r0x = t.r0[0]; d.r0y = t.r0[1]; d.r0z = t.r0[2]; d.mat_in = t.material_in;
+		d.e1x = t.e1[0]; d.e1y = t.e1[1]; d.e1z = t.e1[2]; d.mat_out = t.material_out;
+		d.e2x = t.e2[0]; d.e2y = t.e2[1]; d.e2z = t.e2[2]; d.pad0 = 0;
+		const float* a = t.e1;
+		const float* b = t.e2;
+		d.nx = a[1] * b[2] - a[2] * b[1];
+		d.ny = a[2] * b[0] - a[0] * b[2];
+		d.nz = a[0] * b[1] - a[1] * b[0];
+		d.pad1 = 0;
+	}
+	return out;
+}
+
+// Geometry resident on one device.
+struct DeviceGeometry {
+	DevBuf octree, tris;
+	DevGeometry view{};
+	void upload(const HostGeometry& g, cudaStream_t s)
+	{
+		const std::vector<DevTriangle> dt = device_triangles(g.tris);
+		octree.alloc(g.octree.size() * sizeof(int32_t));
+		tris.alloc(std::max<size_t>(dt.size(), 1) * sizeof(DevTriangle));
+		CU(cudaMemcpyAsync(octree.p, g.octree.data(), g.octree.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+		if (!dt.empty())
+			CU(cudaMemcpyAsync(tris.p, dt.data(), dt.size() * sizeof(DevTriangle), cudaMemcpyHostToDevice, s));
+		CU(cudaStreamSynchronize(s));
+		view.octree = octree.as<int32_t>();
+		view.tris = tris.as<DevTriangle>();
+		view.cx = g.center[0]; view.cy = g.center[1]; view.cz = g.center[2];
+		view.hx = g.halfsize[0]; view.hy = g.halfsize[1]; view.hz = g.halfsize[2];
+		view.max_extent = g.max_extent;
+		view.n_tri = (int32_t)g.tris.size();
+		view.n_octree = (int64_t)g.octree.size();
+	}
+};
+
+// Materials resident on one device: one buffer of all tables plus the
+// DevMaterial array pointing into it.
+struct DeviceMaterials {
+	DevBuf tables, mats;
+	int n = 0;
+	void upload(const std::vector<const HostMaterial*>& ms, cudaStream_t s)
+	{
+		n = (int)ms.size();
+		std::vector<float> blob;
+		std::vector<size_t> offs;
+		auto add = [&](const HostTable& t) {
+			size_t o = blob.size();
+			o = (o + 31) & ~size_t(31);   // 128-byte aligned tables
+			blob.resize(o);
+			offs.push_back(o);
+			blob.insert(blob.end(), t.data.begin(), t.data.end());
+		};
+		for (const HostMaterial* m : ms) {
+			add(m->el_imfp); add(m->el_icdf); add(m->in_imfp); add(m->in_omega); add(m->in_q); add(m->in_binding);
+		}
+		tables.alloc(std::max<size_t>(blob.size(), 1) * sizeof(float));
+		CU(cudaMemcpyAsync(tables.p, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+		std::vector<DevMaterial> dm(ms.size());
+		const float* base = tables.as<float>();
+		size_t k = 0;
+		auto dev = [&](const HostTable& t) {
+			DevTable d;
+			d.data = base + offs[k++];
+			d.nx = t.nx; d.ny = t.ny; d.nz = t.nz; d.pad = 0;
+			d.x_min = t.x_min; d.x_step = t.x_step; d.y_min = t.y_min; d.y_step = t.y_step;
+			d.z_min = t.z_min; d.z_step = t.z_step;
+			return d;
+		};
+		for (size_t i = 0; i < ms.size(); ++i) {
+			const HostMaterial& m = *ms[i];
+			DevMaterial& d = dm[i];
+			d.el_imfp = dev(m.el_imfp); d.el_icdf = dev(m.el_icdf); d.in_imfp = dev(m.in_imfp);
+			d.in_omega = dev(m.in_omega); d.in_q = dev(m.in_q); d.in_binding = dev(m.in_binding);
+			d.fermi = m.fermi; d.band_gap = m.band_gap; d.barrier = m.barrier;
+			d.phonon_loss = m.phonon_loss; d.recoil_const = m.recoil_const;
+			d.in_scale = 1.0f; d.el_scale = 1.0f; d.pad = 0;
+		}
+		mats.alloc(std::max<size_t>(dm.size(), 1) * sizeof(DevMaterial));
+		CU(cudaMemcpyAsync(mats.p, dm.data(), dm.size() * sizeof(DevMaterial), cudaMemcpyHostToDevice, s));
+		CU(cudaStreamSynchronize(s));
+	}
+};
+
+void check_table(const nbl_table& t, int rank, const char* name)
+{
+	require(t.data != nullptr, std::string("table ") + name + " has no data");
+	require(t.nx >= 2 && t.ny >= 1 && t.nz >= 1, std::string("table ") + name + " too small");
+	if (rank >= 2) require(t.ny >= 2, std::string("table ") + name + " needs >= 2 rows");
+	if (rank >= 3) require(t.nz >= 2, std::string("table ") + name + " needs >= 2 planes");
+	if (rank < 3) require(t.nz == 1, std::string("table ") + name + " has the wrong rank");
+	if (rank < 2) require(t.ny == 1, std::string("table ") + name + " has the wrong rank");
+}
+
+HostTable copy_table(const nbl_table& t)
+{
+	HostTable h;
+	h.nx = t.nx; h.ny = t.ny; h.nz = t.nz;
+	h.x_min = t.x_min; h.x_step = t.x_step; h.y_min = t.y_min; h.y_step = t.y_step; h.z_min = t.z_min; h.z_step = t.z_step;
+	h.data.assign(t.data, t.data + (size_t)t.nx * t.ny * t.nz);
+	return h;
+}
+
+}  // namespace
+}  // namespace nbl
+
+/* ======================================================================= */
+/* simulation object                                                        */
+struct nbl_sim {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	bool own_stream = false;
+	nbl_params params{};
+	DeviceGeometry geom;
+	DeviceMaterials mats;
+	DevBuf queues[2][N_QUEUES][6];
+	DevBuf ctrl, counters, detected, n_detected, se_img, bse_img, hist, grad_se, grad_bse;
+	DevBuf primaries;
+	uint64_t pri_cap = 0, n_pri = 0;
+	StepParams sp{};
+	int grid = 0, block = 256;
+	uint32_t graph_iters = 24;
+	uint64_t iteration = 0;
+	cudaGraphExec_t graph = nullptr;
+	bool graph_dirty = true;
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	double kernel_ms = 0;
+	std::vector<nbl_record> host_records;   // records drained from the device during runs
+	uint32_t* pinned_ctrl = nullptr;
+
+	~nbl_sim()
+	{
+		if (graph) cudaGraphExecDestroy(graph);
+		if (ev0) cudaEventDestroy(ev0);
+		if (ev1) cudaEventDestroy(ev1);
+		if (pinned_ctrl) cudaFreeHost(pinned_ctrl);
+		if (own_stream && stream) cudaStreamDestroy(stream);
+	}
+
+	void build_graph()
+	{
+		if (graph) {
+			cudaGraphExecDestroy(graph);
+			graph = nullptr;
+		}
+		cudaGraph_t g = nullptr;
+		CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+		cudaError_t err = cudaSuccess;
+		for (uint32_t i = 0; i < graph_iters && err == cudaSuccess; ++i)
+			err = launch_step(sp, i, grid, block, stream);
+		cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+		CU(err);
+		CU(e2);
+		err = cudaGraphInstantiate(&graph, g, 0);
+		cudaGraphDestroy(g);
+		CU(err);
+		graph_dirty = false;
+	}
+
+	// Launch one graph of `graph_iters` iterations (iteration index is a
+	// multiple of 6 here, so the rotating slots and queue parity line up).
+	void launch_graph()
+	{
+		if (graph_dirty)
+			build_graph();
+		CU(cudaEventRecord(ev0, stream));
+		CU(cudaGraphLaunch(graph, stream));
+		CU(cudaEventRecord(ev1, stream));
+		iteration += graph_iters;
+	}
+
+	// Queue counts + cursor of the next iteration's read slot.
+	void read_ctrl(uint32_t out[SLOT_WORDS])
+	{
+		const uint32_t slot = (uint32_t)(iteration % 3);
+		CU(cudaMemcpyAsync(pinned_ctrl, ctrl.as<uint32_t>() + slot * SLOT_WORDS, SLOT_WORDS * sizeof(uint32_t),
+			cudaMemcpyDeviceToHost, stream));
+		CU(cudaMemcpyAsync(pinned_ctrl + SLOT_WORDS, n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+		CU(cudaStreamSynchronize(stream));
+		float ms = 0;
+		if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess)
+			kernel_ms += ms;
+		std::memcpy(out, pinned_ctrl, SLOT_WORDS * sizeof(uint32_t));
+	}
+
+	// Move device records to the host store.
+	void drain_to_host(uint32_t n_dev)
+	{
+		const uint32_t n = std::min(n_dev, sp.det_cap);
+		if (n == 0) return;
+		const size_t old = host_records.size();
+		host_records.resize(old + n);
+		CU(cudaMemcpyAsync(host_records.data() + old, detected.p, (size_t)n * sizeof(nbl_record), cudaMemcpyDeviceToHost, stream));
+		CU(cudaMemsetAsync(n_detected.p, 0, sizeof(uint32_t), stream));
+		CU(cudaStreamSynchronize(stream));
+	}
+
+	// Run graphs until done (or `max_graphs` graphs); returns electrons still
+	// in flight plus primaries not yet started.
+	int64_t advance(uint64_t max_graphs)
+	{
+		uint32_t c[SLOT_WORDS + 1];
+		for (uint64_t k = 0; k < max_graphs; ++k) {
+			launch_graph();
+			read_ctrl(c);
+			const uint32_t ndet = pinned_ctrl[SLOT_WORDS];
+			if (ndet > sp.det_cap / 4)
+				drain_to_host(ndet);
+			const uint64_t active = (uint64_t)c[0] + c[1] + c[2] + c[3];
+			const uint64_t left = n_pri - c[SLOT_CURSOR];
+			if (active == 0 && left == 0)
+				return 0;
+		}
+		read_ctrl(c);
+		return (int64_t)((uint64_t)c[0] + c[1] + c[2] + c[3] + (n_pri - c[SLOT_CURSOR]));
+	}
+
+	void check_errors()
+	{
+		unsigned long long cnt[N_COUNTERS];
+		CU(cudaMemcpyAsync(cnt, counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
+		CU(cudaStreamSynchronize(stream));
+		if (cnt[CNT_QUEUE_OVERFLOW] || cnt[CNT_RECORD_OVERFLOW])
+			throw Error(NBL_ERR_POOL_OVERFLOW, "event queue or record buffer overflowed (" +
+				std::to_string(cnt[CNT_QUEUE_OVERFLOW]) + " electrons, " + std::to_string(cnt[CNT_RECORD_OVERFLOW]) +
+				" records dropped); raise capacity / record_capacity");
+		if (cnt[CNT_NAN])
+			throw Error(NBL_ERR_NAN_STATE, std::to_string(cnt[CNT_NAN]) + " electrons reached a NaN state");
+		if (cnt[CNT_EVENT_BUDGET] || cnt[CNT_WALK_OVERFLOW])
+			throw Error(NBL_ERR_BUDGET_EXCEEDED, std::to_string(cnt[CNT_EVENT_BUDGET]) +
+				" electrons exceeded the event budget, " + std::to_string(cnt[CNT_WALK_OVERFLOW]) + " octree walks the step bound");
+	}
+
+	void reset_device_state()
+	{
+		CU(cudaMemsetAsync(ctrl.p, 0, ctrl.bytes, stream));
+		CU(cudaMemsetAsync(counters.p, 0, counters.bytes, stream));
+		CU(cudaMemsetAsync(n_detected.p, 0, n_detected.bytes, stream));
+		if (se_img.p) CU(cudaMemsetAsync(se_img.p, 0, se_img.bytes, stream));
+		if (bse_img.p) CU(cudaMemsetAsync(bse_img.p, 0, bse_img.bytes, stream));
+		if (hist.p) CU(cudaMemsetAsync(hist.p, 0, hist.bytes, stream));
+		if (grad_se.p) CU(cudaMemsetAsync(grad_se.p, 0, grad_se.bytes, stream));
+		if (grad_bse.p) CU(cudaMemsetAsync(grad_bse.p, 0, grad_bse.bytes, stream));
+		CU(cudaStreamSynchronize(stream));
+		iteration = 0;
+		kernel_ms = 0;
+		host_records.clear();
+	}
+
+	void ensure_primary_capacity(uint64_t need)
+	{
+		if (need <= pri_cap) return;
+		uint64_t cap = std::max<uint64_t>(need, pri_cap * 2);
+		cap = std::max<uint64_t>(cap, 1024);
+		DevBuf nb(cap * sizeof(Record36));
+		if (n_pri)
+			CU(cudaMemcpyAsync(nb.p, primaries.p, n_pri * sizeof(Record36), cudaMemcpyDeviceToDevice, stream));
+		CU(cudaStreamSynchronize(stream));
+		std::swap(primaries.p, nb.p);
+		std::swap(primaries.bytes, nb.bytes);
+		pri_cap = cap;
+		sp.primaries = primaries.as<Record36>();
+		graph_dirty = true;
+	}
+};
+
+/* ======================================================================= */
+extern "C" {
+
+const char* nbl_last_error_string(void) { return g_last_error.c_str(); }
+int nbl_abi_version(void) { return NBL_ABI_VERSION; }
+void nbl_free(void* p) { std::free(p); }
+
+nbl_status nbl_load_tri_file(const char* path, nbl_triangle** out, int64_t* n)
+{
+	return guard([&] {
+		require(path && out && n, "null argument");
+		std::ifstream f(path);
+		require(bool(f), std::string("cannot open ") + path, NBL_ERR_IO);
+		std::vector<nbl_triangle> v;
+		std::string line;
+		size_t line_num = 0;
+		while (std::getline(f, line)) {
+			++line_num;
+			const size_t i = line.find_first_not_of(" \t\r");
+			if (i == std::string::npos || line[i] == '#')
+				continue;
+			std::istringstream ss(line);
+			std::vector<std::string> cols;
+			std::string c;
+			while (ss >> c) cols.push_back(c);
+			require(cols.size() == 11, "invalid number of columns in line " + std::to_string(line_num), NBL_ERR_IO);
+			nbl_triangle t;
+			t.material_in = std::stoi(cols[0]);
+			t.material_out = std::stoi(cols[1]);
+			float r[3][3];
+			for (int k = 0; k < 9; ++k) r[k / 3][k % 3] = (float)std::stod(cols[2 + k]);
+			for (int k = 0; k < 3; ++k) {
+				t.r0[k] = r[0][k];
+				t.e1[k] = r[1][k] - r[0][k];
+				t.e2[k] = r[2][k] - r[0][k];
+			}
+			v.push_back(t);
+		}
+		*n = (int64_t)v.size();
+		*out = static_cast<nbl_triangle*>(std::malloc(std::max<size_t>(v.size(), 1) * sizeof(nbl_triangle)));
+		if (!*out) throw std::bad_alloc();
+		std::memcpy(*out, v.data(), v.size() * sizeof(nbl_triangle));
+	});
+}
+
+nbl_status nbl_load_pri_file(const char* path, nbl_record** out, int64_t* n)
+{
+	return guard([&] {
+		require(path && out && n, "null argument");
+		std::ifstream f(path, std::ios::binary | std::ios::ate);
+		require(bool(f), std::string("cannot open ") + path, NBL_ERR_IO);
+		const std::streamsize sz = f.tellg();
+		require(sz % 36 == 0, "Unexpected end of primaries file", NBL_ERR_IO);
+		f.seekg(0);
+		*n = sz / 36;
+		*out = static_cast<nbl_record*>(std::malloc(std::max<std::streamsize>(sz, 1)));
+		if (!*out) throw std::bad_alloc();
+		f.read(reinterpret_cast<char*>(*out), sz);
+	});
+}
+
+/* materials */
+nbl_status nbl_material_load(const char* path, nbl_material** out)
+{
+	return guard([&] {
+		require(path && out, "null argument");
+		auto m = std::make_unique<nbl_material>();
+		m->m = load_material_file(path);
+		*out = m.release();
+	});
+}
+
+nbl_status nbl_material_create(const nbl_material_tables* t, nbl_material** out)
+{
+	return guard([&] {
+		require(t && out, "null argument");
+		check_table(t->el_imfp, 1, "el_imfp"); check_table(t->el_icdf, 2, "el_icdf");
+		check_table(t->in_imfp, 1, "in_imfp"); check_table(t->in_omega, 2, "in_omega");
+		check_table(t->in_q, 3, "in_q"); check_table(t->in_binding, 3, "in_binding");
+		auto m = std::make_unique<nbl_material>();
+		m->m.el_imfp = copy_table(t->el_imfp); m->m.el_icdf = copy_table(t->el_icdf);
+		m->m.in_imfp = copy_table(t->in_imfp); m->m.in_omega = copy_table(t->in_omega);
+		m->m.in_q = copy_table(t->in_q); m->m.in_binding = copy_table(t->in_binding);
+		m->m.fermi = t->fermi; m->m.band_gap = t->band_gap; m->m.barrier = t->barrier;
+		m->m.phonon_loss = t->phonon_loss; m->m.recoil_const = t->recoil_const;
+		*out = m.release();
+	});
+}
+
+nbl_status nbl_material_get_tables(const nbl_material* m, nbl_material_tables* out)
+{
+	return guard([&] {
+		require(m && out, "null argument");
+		out->el_imfp = m->m.el_imfp.view(); out->el_icdf = m->m.el_icdf.view();
+		out->in_imfp = m->m.in_imfp.view(); out->in_omega = m->m.in_omega.view();
+		out->in_q = m->m.in_q.view(); out->in_binding = m->m.in_binding.view();
+		out->fermi = m->m.fermi; out->band_gap = m->m.band_gap; out->barrier = m->m.barrier;
+		out->phonon_loss = m->m.phonon_loss; out->recoil_const = m->m.recoil_const;
+	});
+}
+
+nbl_status nbl_material_max_energy(const nbl_material* m, float* out)
+{
+	return guard([&] {
+		require(m && out, "null argument");
+		// get_max_energy: exp of the last IMFP abscissa (full_penn.h:42-45, elastic.h:46-49)
+		auto emax = [](const HostTable& t) { return std::exp(t.x_min + (t.nx - 1) / t.x_step); };
+		*out = std::min(emax(m->m.in_imfp), emax(m->m.el_imfp));
+	});
+}
+
+void nbl_material_destroy(nbl_material* m) { delete m; }
+
+/* geometry */
+nbl_status nbl_geometry_build(const nbl_triangle* tris, int64_t n, int32_t max_depth, int32_t split_count,
+	nbl_geometry** out)
+{
+	return guard([&] {
+		require(tris && out, "null argument");
+		auto g = std::make_unique<nbl_geometry>();
+		g->g = build_octree(tris, n, max_depth, split_count);
+		*out = g.release();
+	});
+}
+
+nbl_status nbl_geometry_from_linearized(const int32_t* octree_data, int64_t n_octree, const nbl_triangle* tris,
+	int64_t n_tri, const float center[3], const float halfsize[3], nbl_geometry** out)
+{
+	return guard([&] {
+		require(octree_data && tris && center && halfsize && out, "null argument");
+		require(n_octree >= 9 && n_tri >= 0, "octree too small");
+		// validate the whole structure so that no walk can read out of bounds:
+		// inner nodes hold 8 in-range child offsets, leaves a -1 terminated
+		// list of triangle ids, depth <= 21 (63-bit location codes)
+		{
+			std::vector<uint8_t> seen((size_t)n_octree, 0);
+			std::vector<std::pair<int64_t, int>> stack{ { 0, 0 } };
+			while (!stack.empty()) {
+				const int64_t at = stack.back().first;
+				const int depth = stack.back().second;
+				stack.pop_back();
+				require(at >= 0 && at + 8 <= n_octree, "octree inner node out of range");
+				require(!seen[at], "octree has a shared or cyclic node");
+				seen[at] = 1;
+				require(depth < 21, "octree deeper than 21 levels");
+				for (int o = 0; o < 8; ++o) {
+					const int64_t v = octree_data[at + o];
+					require(v != 0, "octree child offset is zero");
+					if (v > 0) {
+						stack.push_back({ v, depth + 1 });
+					} else {
+						int64_t k = -v;
+						for (;; ++k) {
+							require(k < n_octree, "octree leaf runs past the end");
+							const int32_t t = octree_data[k];
+							if (t < 0) {
+								require(t == -1, "octree leaf must end with -1");
+								break;
+							}
+							require(t < n_tri, "octree leaf names a triangle out of range");
+						}
+					}
+				}
+			}
+		}
+		auto g = std::make_unique<nbl_geometry>();
+		g->g.octree.assign(octree_data, octree_data + n_octree);
+		g->g.tris.assign(tris, tris + n_tri);
+		for (int k = 0; k < 3; ++k) {
+			g->g.center[k] = center[k];
+			g->g.halfsize[k] = halfsize[k];
+		}
+		g->g.max_extent = max_extent_of(g->g.halfsize);
+		*out = g.release();
+	});
+}
+
+nbl_status nbl_geometry_info(const nbl_geometry* g, int64_t* n_octree, int64_t* n_tri, float center[3],
+	float halfsize[3], float* max_extent)
+{
+	return guard([&] {
+		require(g != nullptr, "null geometry");
+		if (n_octree) *n_octree = (int64_t)g->g.octree.size();
+		if (n_tri) *n_tri = (int64_t)g->g.tris.size();
+		for (int k = 0; k < 3; ++k) {
+			if (center) center[k] = g->g.center[k];
+			if (halfsize) halfsize[k] = g->g.halfsize[k];
+		}
+		if (max_extent) *max_extent = g->g.max_extent;
+	});
+}
+
+nbl_status nbl_geometry_export(const nbl_geometry* g, int32_t* octree_data, nbl_triangle* tris)
+{
+	return guard([&] {
+		require(g != nullptr, "null geometry");
+		if (octree_data) std::memcpy(octree_data, g->g.octree.data(), g->g.octree.size() * sizeof(int32_t));
+		if (tris) std::memcpy(tris, g->g.tris.data(), g->g.tris.size() * sizeof(nbl_triangle));
+	});
+}
+
+void nbl_geometry_destroy(nbl_geometry* g)
+{
+	if (!g) return;
+	for (auto& kv : g->dev) {
+		if (cudaSetDevice(kv.first) == cudaSuccess) {
+			cudaFree(kv.second.octree);
+			cudaFree(kv.second.tris);
+		}
+	}
+	delete g;
+}
+
+nbl_status nbl_ray_query(const nbl_geometry* g, int device, int64_t n, const float* pos, const float* dir,
+	const float* dist, const int32_t* ignore_tri, const int32_t* ignore_mat, float* out_dist, int32_t* out_tri)
+{
+	return guard([&] {
+		require(g && pos && dir && dist && ignore_tri && ignore_mat && out_dist && out_tri, "null argument");
+		require(n >= 0, "negative count");
+		for (int64_t i = 0; i < n; ++i)
+			require(ignore_tri[i] < (int64_t)g->g.tris.size(), "ignore_tri out of range");
+		set_device(device);
+		if (n == 0) return;
+		cudaStream_t s;
+		CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+		struct S { cudaStream_t s; ~S() { cudaStreamDestroy(s); } } sg{ s };
+		DeviceGeometry dg;
+		dg.upload(g->g, s);
+		DevBuf b(n * (3 * 4 + 3 * 4 + 4 + 4 + 4 + 4 + 4));
+		char* p = b.as<char>();
+		float* d_pos = (float*)p; p += n * 12;
+		float* d_dir = (float*)p; p += n * 12;
+		float* d_dist = (float*)p; p += n * 4;
+		int32_t* d_it = (int32_t*)p; p += n * 4;
+		int32_t* d_im = (int32_t*)p; p += n * 4;
+		float* d_od = (float*)p; p += n * 4;
+		int32_t* d_ot = (int32_t*)p;
+		CU(cudaMemcpyAsync(d_pos, pos, n * 12, cudaMemcpyHostToDevice, s));
+		CU(cudaMemcpyAsync(d_dir, dir, n * 12, cudaMemcpyHostToDevice, s));
+		CU(cudaMemcpyAsync(d_dist, dist, n * 4, cudaMemcpyHostToDevice, s));
+		CU(cudaMemcpyAsync(d_it, ignore_tri, n * 4, cudaMemcpyHostToDevice, s));
+		CU(cudaMemcpyAsync(d_im, ignore_mat, n * 4, cudaMemcpyHostToDevice, s));
+		CU(launch_ray_query(dg.view, d_pos, d_dir, d_dist, d_it, d_im, n, d_od, d_ot, s));
+		CU(cudaMemcpyAsync(out_dist, d_od, n * 4, cudaMemcpyDeviceToHost, s));
+		CU(cudaMemcpyAsync(out_tri, d_ot, n * 4, cudaMemcpyDeviceToHost, s));
+		CU(cudaStreamSynchronize(s));
+	});
+}
+
+void nbl_physics_defaults(nbl_physics_opts* o)
+{
+	if (!o) return;
+	o->inelastic_model = 0;
+	o->generate_secondaries = 1;
+	o->acoustic_phonon_loss = 1;
+	o->atomic_recoil_loss = 1;
+	o->quantum_transmission = 1;
+	o->interface_refraction = 1;
+	o->interface_absorption = 0;
+}
+
+void nbl_params_defaults(nbl_params* p)
+{
+	if (!p) return;
+	std::memset(p, 0, sizeof(*p));
+	p->seed = 0x78c7e39bull;   // gpu_main.cu --seed default
+	nbl_physics_defaults(&p->physics);
+}
+
+nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
+	const nbl_params* params, nbl_sim** out)
+{
+	return guard([&] {
+		require(g && materials && params && out, "null argument");
+		require(n_materials >= 1 && n_materials <= 127, "need 1..127 materials");
+		const nbl_physics_opts& ph = params->physics;
+		require(ph.inelastic_model == 0 && ph.generate_secondaries == 1 && ph.acoustic_phonon_loss == 1 &&
+			ph.atomic_recoil_loss == 1 && ph.quantum_transmission == 1 && ph.interface_refraction == 1 &&
+			ph.interface_absorption == 0,
+			"only the reference's default physics selection (physics_config.h) is built");
+		int max_mat = -1;
+		for (const nbl_triangle& t : g->g.tris)
+			max_mat = std::max(max_mat, std::max(t.material_in, t.material_out));
+		require(max_mat < n_materials, "geometry uses material " + std::to_string(max_mat) + " but only " +
+			std::to_string(n_materials) + " materials were given");
+		require(params->adjoint == 0 || n_materials <= 2, "the adjoint covers at most 2 materials (6 parameters)");
+
+		auto s = std::make_unique<nbl_sim>();
+		s->params = *params;
+		s->device = params->device;
+		set_device(s->device);
+		if (params->stream) {
+			s->stream = static_cast<cudaStream_t>(params->stream);
+		} else {
+			CU(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+			s->own_stream = true;
+		}
+		CU(cudaEventCreate(&s->ev0));
+		CU(cudaEventCreate(&s->ev1));
+		CU(cudaMallocHost(&s->pinned_ctrl, (SLOT_WORDS + 4) * sizeof(uint32_t)));
+
+		const uint32_t cap = params->capacity ? params->capacity : (1u << 20);
+		require(cap >= 32 && cap <= (1u << 28), "capacity must be 32..2^28");
+		s->block = params->block_size ? (int)params->block_size : 256;
+		require(s->block % 32 == 0 && s->block >= 32 && s->block <= 256, "block_size must be a multiple of 32 in 32..256");
+		s->grid = params->grid_size ? (int)params->grid_size : step_grid_size(s->device, s->block);
+		uint32_t gi = params->iterations_per_graph ? params->iterations_per_graph : 24;
+		gi = (gi + 5) / 6 * 6;
+		s->graph_iters = gi;
+
+		s->geom.upload(g->g, s->stream);
+		std::vector<const HostMaterial*> ms;
+		for (int i = 0; i < n_materials; ++i) {
+			require(materials[i] != nullptr, "null material");
+			ms.push_back(&materials[i]->m);
+		}
+		s->mats.upload(ms, s->stream);
+
+		StepParams& sp = s->sp;
+		sp.geom = s->geom.view;
+		sp.mats = s->mats.mats.as<DevMaterial>();
+		sp.n_mat = n_materials;
+		sp.energy_threshold = params->energy_threshold;
+		sp.key.k0 = (uint32_t)params->seed;
+		sp.key.k1 = (uint32_t)(params->seed >> 32);
+		sp.capacity = cap;
+		sp.qcap = 2 * cap;
+		const bool adj = params->adjoint != 0;
+		for (int b = 0; b < 2; ++b)
+			for (int q = 0; q < N_QUEUES; ++q) {
+				DevBuf* qb = s->queues[b][q];
+				qb[0].alloc((size_t)sp.qcap * sizeof(float4));
+				qb[1].alloc((size_t)sp.qcap * sizeof(float4));
+				qb[2].alloc((size_t)sp.qcap * sizeof(uint4));
+				qb[3].alloc((size_t)sp.qcap * sizeof(uint32_t));
+				if (adj) {
+					qb[4].alloc((size_t)sp.qcap * sizeof(float4));
+					qb[5].alloc((size_t)sp.qcap * sizeof(float2));
+				}
+				Queue& Q = sp.q[b][q];
+				Q.a = qb[0].as<float4>(); Q.b = qb[1].as<float4>(); Q.c = qb[2].as<uint4>(); Q.d = qb[3].as<uint32_t>();
+				Q.s = qb[4].as<float4>(); Q.s2 = qb[5].as<float2>();
+			}
+		s->ctrl.alloc(3 * SLOT_WORDS * sizeof(uint32_t));
+		sp.ctrl = s->ctrl.as<uint32_t>();
+		s->counters.alloc(N_COUNTERS * sizeof(unsigned long long));
+		sp.counters = s->counters.as<unsigned long long>();
+		sp.det_cap = params->record_capacity ? params->record_capacity : std::max<uint32_t>(4 * cap, 1u << 20);
+		s->detected.alloc((size_t)sp.det_cap * sizeof(Record36));
+		sp.detected = s->detected.as<Record36>();
+		s->n_detected.alloc(sizeof(uint32_t));
+		sp.n_detected = s->n_detected.as<uint32_t>();
+		Tallies& T = sp.tal;
+		T.nx = params->tally_nx; T.ny = params->tally_ny;
+		require(T.nx >= 0 && T.ny >= 0 && (int64_t)T.nx * T.ny < (int64_t)1 << 28, "tally grid too large");
+		if (T.nx > 0 && T.ny > 0) {
+			const size_t np = (size_t)T.nx * T.ny;
+			s->se_img.alloc(np * sizeof(uint32_t));
+			s->bse_img.alloc(np * sizeof(uint32_t));
+			T.se_img = s->se_img.as<uint32_t>();
+			T.bse_img = s->bse_img.as<uint32_t>();
+			if (adj) {
+				s->grad_se.alloc(np * 6 * sizeof(double));
+				s->grad_bse.alloc(np * 6 * sizeof(double));
+				T.grad_se = s->grad_se.as<double>();
+				T.grad_bse = s->grad_bse.as<double>();
+			}
+		}
+		T.n_bins = params->hist_bins > 0 ? params->hist_bins : 200;
+		T.hist_emax = params->hist_emax > 0 ? params->hist_emax : 1000.0f;
+		s->hist.alloc((size_t)T.n_bins * sizeof(uint32_t));
+		T.hist = s->hist.as<uint32_t>();
+		sp.max_events = params->max_events ? params->max_events : (1u << 22);
+		require(sp.max_events < (1u << 24), "max_events must be < 2^24");
+		sp.adjoint = adj ? 1 : 0;
+		s->ensure_primary_capacity(1024);
+		sp.n_primaries = 0;
+		s->reset_device_state();
+		*out = s.release();
+	});
+}
+
+static void push_common(nbl_sim* s, const void* src, int64_t n, cudaMemcpyKind kind)
+{
+	require(s != nullptr, "null simulation");
+	require(n >= 0, "negative count");
+	require(s->n_pri + (uint64_t)n < 0xFFFFFFFFull, "at most 2^32-1 primaries per simulation");
+	if (n == 0) return;
+	set_device(s->device);
+	s->ensure_primary_capacity(s->n_pri + n);
+	CU(cudaMemcpyAsync(s->primaries.as<Record36>() + s->n_pri, src, (size_t)n * sizeof(Record36), kind, s->stream));
+	CU(cudaStreamSynchronize(s->stream));
+	s->n_pri += n;
+	s->sp.n_primaries = (uint32_t)s->n_pri;
+	s->graph_dirty = true;
+}
+
+nbl_status nbl_sim_push_primaries(nbl_sim* s, const nbl_record* recs, int64_t n)
+{
+	return guard([&] {
+		require(recs != nullptr || n == 0, "null records");
+		push_common(s, recs, n, cudaMemcpyHostToDevice);
+	});
+}
+
+nbl_status nbl_sim_push_primaries_device(nbl_sim* s, const void* d_recs, int64_t n)
+{
+	return guard([&] {
+		require(d_recs != nullptr || n == 0, "null records");
+		push_common(s, d_recs, n, cudaMemcpyDeviceToDevice);
+	});
+}
+
+nbl_status nbl_sim_step(nbl_sim* s, uint32_t iterations, int64_t* running)
+{
+	return guard([&] {
+		require(s != nullptr, "null simulation");
+		set_device(s->device);
+		const uint64_t graphs = (iterations + s->graph_iters - 1) / s->graph_iters;
+		const int64_t r = s->advance(std::max<uint64_t>(graphs, 1));
+		if (running) *running = r;
+		s->check_errors();
+	});
+}
+
+nbl_status nbl_sim_run(nbl_sim* s)
+{
+	return guard([&] {
+		require(s != nullptr, "null simulation");
+		set_device(s->device);
+		// the budget bounds the iterations: an electron cannot outlive
+		// max_events flights, and the pool refills at least one primary per
+		// iteration while primaries are left
+		const uint64_t bound = (uint64_t)s->sp.max_events + s->n_pri + 16;
+		const uint64_t max_graphs = bound / s->graph_iters + 2;
+		const int64_t left = s->advance(max_graphs);
+		s->check_errors();
+		if (left != 0)
+			throw Error(NBL_ERR_BUDGET_EXCEEDED, "run did not finish within its iteration bound");
+	});
+}
+
+nbl_status nbl_sim_detected_count(nbl_sim* s, int64_t* n)
+{
+	return guard([&] {
+		require(s && n, "null argument");
+		set_device(s->device);
+		uint32_t d = 0;
+		CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+		*n = (int64_t)s->host_records.size() + std::min(d, s->sp.det_cap);
+	});
+}
+
+nbl_status nbl_sim_drain_detected(nbl_sim* s, nbl_record* out, int64_t cap, int64_t* n)
+{
+	return guard([&] {
+		require(s && n && (out || cap == 0), "null argument");
+		set_device(s->device);
+		uint32_t d = 0;
+		CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+		if (d) s->drain_to_host(d);
+		const int64_t k = std::min<int64_t>(cap, (int64_t)s->host_records.size());
+		if (k > 0) std::memcpy(out, s->host_records.data(), (size_t)k * sizeof(nbl_record));
+		s->host_records.erase(s->host_records.begin(), s->host_records.begin() + k);
+		*n = k;
+	});
+}
+
+nbl_status nbl_sim_tallies(nbl_sim* s, uint32_t* se_img, uint32_t* bse_img, uint32_t* hist)
+{
+	return guard([&] {
+		require(s != nullptr, "null simulation");
+		set_device(s->device);
+		const Tallies& T = s->sp.tal;
+		if (se_img && s->se_img.p)
+			CU(cudaMemcpyAsync(se_img, s->se_img.p, s->se_img.bytes, cudaMemcpyDeviceToHost, s->stream));
+		if (bse_img && s->bse_img.p)
+			CU(cudaMemcpyAsync(bse_img, s->bse_img.p, s->bse_img.bytes, cudaMemcpyDeviceToHost, s->stream));
+		if (hist)
+			CU(cudaMemcpyAsync(hist, T.hist, (size_t)T.n_bins * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+	});
+}
+
+nbl_status nbl_sim_counters(nbl_sim* s, nbl_counters* out)
+{
+	return guard([&] {
+		require(s && out, "null argument");
+		set_device(s->device);
+		unsigned long long c[N_COUNTERS];
+		uint32_t d = 0;
+		CU(cudaMemcpyAsync(c, s->counters.p, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+		out->flights = c[CNT_FLIGHTS]; out->boundary = c[CNT_BOUNDARY]; out->elastic = c[CNT_ELASTIC];
+		out->inelastic = c[CNT_INELASTIC]; out->spawned = c[CNT_SPAWNED]; out->detected = c[CNT_DETECTED];
+		out->terminated = c[CNT_TERMINATED]; out->primaries_started = c[CNT_PRIMARIES];
+		out->walk_overflow = c[CNT_WALK_OVERFLOW]; out->nan_state = c[CNT_NAN];
+		out->queue_overflow = c[CNT_QUEUE_OVERFLOW]; out->record_overflow = c[CNT_RECORD_OVERFLOW];
+		out->event_budget = c[CNT_EVENT_BUDGET];
+		out->deferred = c[CNT_DEFERRED];
+		out->iterations = s->iteration;
+		out->primaries_total = s->n_pri;
+		out->records_pending = s->host_records.size() + std::min(d, s->sp.det_cap);
+	});
+}
+
+nbl_status nbl_sim_reset(nbl_sim* s)
+{
+	return guard([&] {
+		require(s != nullptr, "null simulation");
+		set_device(s->device);
+		s->n_pri = 0;
+		s->sp.n_primaries = 0;
+		s->graph_dirty = true;
+		s->reset_device_state();
+	});
+}
+
+nbl_status nbl_sim_kernel_ms(nbl_sim* s, double* ms)
+{
+	return guard([&] {
+		require(s && ms, "null argument");
+		*ms = s->kernel_ms;
+	});
+}
+
+void nbl_sim_destroy(nbl_sim* s)
+{
+	if (!s) return;
+	cudaSetDevice(s->device);
+	if (s->stream) cudaStreamSynchronize(s->stream);
+	delete s;
+}
+
+/* debug entry points */
+nbl_status nbl_debug_table_lookup(const nbl_material* m, int device, int32_t which, int32_t rounddown, int64_t n,
+	const float* x, const float* y, const float* z, float* out)
+{
+	return guard([&] {
+		require(m && x && y && z && out, "null argument");
+		require(which >= 0 && which <= 5 && n >= 0, "bad arguments");
+		set_device(device);
+		if (n == 0) return;
+		cudaStream_t s;
+		CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+		struct S { cudaStream_t s; ~S() { cudaStreamDestroy(s); } } sg{ s };
+		DeviceMaterials dm;
+		dm.upload({ &m->m }, s);
+		DevBuf b(n * 16);
+		float* dx = b.as<float>();
+		float* dy = dx + n;
+		float* dz = dy + n;
+		float* dout = dz + n;
+		CU(cudaMemcpyAsync(dx, x, n * 4, cudaMemcpyHostToDevice, s));
+		CU(cudaMemcpyAsync(dy, y, n * 4, cudaMemcpyHostToDevice, s));
+		CU(cudaMemcpyAsync(dz, z, n * 4, cudaMemcpyHostToDevice, s));
+		CU(launch_table_kat(dm.mats.as<DevMaterial>(), which, rounddown, n, dx, dy, dz, dout, s));
+		CU(cudaMemcpyAsync(out, dout, n * 4, cudaMemcpyDeviceToHost, s));
+		CU(cudaStreamSynchronize(s));
+	});
+}
+
+nbl_status nbl_debug_event(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials, int device,
+	int32_t kind, int64_t n, const float* state_in, const int32_t* mat_in, const int32_t* tri, const float* uniforms,
+	int32_t n_uniforms, float* state_out, int32_t* mat_out, int32_t* status, float* se_out, int32_t* has_se,
+	int32_t* used)
+{
+	return guard([&] {
+		require(materials && state_in && mat_in && uniforms && state_out && mat_out && status && se_out && has_se && used,
+			"null argument");
+		require(kind >= 1 && kind <= 3 && n >= 0 && n_uniforms > 0 && n_materials >= 1, "bad arguments");
+		if (kind == 3) {
+			require(g && tri, "boundary events need a geometry and triangles");
+			for (int64_t i = 0; i < n; ++i)
+				require(tri[i] >= 0 && tri[i] < (int64_t)g->g.tris.size(), "triangle index out of range");
+		} else {
+			for (int64_t i = 0; i < n; ++i)
+				require(mat_in[i] >= 0 && mat_in[i] < n_materials, "scatter events need a physical material");
+		}
+		set_device(device);
+		if (n == 0) return;
+		cudaStream_t s;
+		CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+		struct S { cudaStream_t s; ~S() { cudaStreamDestroy(s); } } sg{ s };
+		std::vector<const HostMaterial*> ms;
+		for (int i = 0; i < n_materials; ++i) ms.push_back(&materials[i]->m);
+		DeviceMaterials dm;
+		dm.upload(ms, s);
+		DeviceGeometry dg;
+		if (g) dg.upload(g->g, s);
+		const size_t nu = (size_t)n * n_uniforms;
+		DevBuf b(n * (7 * 4 * 3 + 4 * 6) + nu * 4);
+		char* p = b.as<char>();
+		float* d_si = (float*)p; p += n * 28;
+		float* d_so = (float*)p; p += n * 28;
+		float* d_se = (float*)p; p += n * 28;
+		int32_t* d_mi = (int32_t*)p; p += n * 4;
+		int32_t* d_tri = (int32_t*)p; p += n * 4;
+		int32_t* d_mo = (int32_t*)p; p += n * 4;
+		int32_t* d_st = (int32_t*)p; p += n * 4;
+		int32_t* d_hs = (int32_t*)p; p += n * 4;
+		int32_t* d_us = (int32_t*)p; p += n * 4;
+		float* d_u = (float*)p;
+		CU(cudaMemcpyAsync(d_si, state_in, n * 28, cudaMemcpyHostToDevice, s));
+		CU(cudaMemcpyAsync(d_mi, mat_in, n * 4, cudaMemcpyHostToDevice, s));
+		if (tri) CU(cudaMemcpyAsync(d_tri, tri, n * 4, cudaMemcpyHostToDevice, s));
+		else CU(cudaMemsetAsync(d_tri, 0, n * 4, s));
+		CU(cudaMemcpyAsync(d_u, uniforms, nu * 4, cudaMemcpyHostToDevice, s));
+		CU(launch_event_kat(dg.view, dm.mats.as<DevMaterial>(), kind, n, d_si, d_mi, d_tri, d_u, n_uniforms, d_so, d_mo,
+			d_st, d_se, d_hs, d_us, s));
+		CU(cudaMemcpyAsync(state_out, d_so, n * 28, cudaMemcpyDeviceToHost, s));
+		CU(cudaMemcpyAsync(mat_out, d_mo, n * 4, cudaMemcpyDeviceToHost, s));
+		CU(cudaMemcpyAsync(status, d_st, n * 4, cudaMemcpyDeviceToHost, s));
+		CU(cudaMemcpyAsync(se_out, d_se, n * 28, cudaMemcpyDeviceToHost, s));
+		CU(cudaMemcpyAsync(has_se, d_hs, n * 4, cudaMemcpyDeviceToHost, s));
+		CU(cudaMemcpyAsync(used, d_us, n * 4, cudaMemcpyDeviceToHost, s));
+		CU(cudaStreamSynchronize(s));
+	});
+}
+
+}  // extern "C"

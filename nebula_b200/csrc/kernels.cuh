@@ -1,0 +1,80 @@
+// Host-visible declarations of the device-side run state and the kernel
+// launchers (implemented in transport.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "nbl_device_types.h"
+
+namespace nbl {
+
+// Electron state in structure-of-arrays form, one set per queue.  Three
+// 16-byte vectors and one word per electron (52 B), so each field of a warp's
+// 32 electrons is one fully coalesced 512-byte transaction.
+struct Queue {
+	float4* a;      // x, y, z, kinetic energy (eV)
+	float4* b;      // direction x, y, z (unnormalised), material id (int bits)
+	uint4* c;       // last triangle (-1 none), primary tag, event counter, lineage lo
+	uint32_t* d;    // lineage hi
+	float4* s;      // adjoint: scores d log p / d theta, parameters 0..3 (null if off)
+	float2* s2;     // adjoint: parameters 4..5
+};
+
+// Counters kept on the device (64-bit).
+enum : int {
+	CNT_FLIGHTS = 0, CNT_BOUNDARY, CNT_ELASTIC, CNT_INELASTIC, CNT_SPAWNED, CNT_DETECTED,
+	CNT_TERMINATED, CNT_PRIMARIES, CNT_WALK_OVERFLOW, CNT_NAN, CNT_QUEUE_OVERFLOW,
+	CNT_RECORD_OVERFLOW, CNT_EVENT_BUDGET, CNT_DEFERRED, N_COUNTERS
+};
+
+// Per-iteration control words, three rotating slots of 8 words:
+// [queue counts x4, primary cursor, secondary tickets, pad x2].
+constexpr int SLOT_WORDS = 8;
+constexpr int SLOT_CURSOR = 4;
+constexpr int SLOT_TICKETS = 5;
+
+struct Tallies {
+	uint32_t* se_img;        // per pixel counts of detected E < 50 eV (null: off)
+	uint32_t* bse_img;       // per pixel counts of detected E >= 50 eV
+	uint32_t* hist;          // energy histogram [n_bins]
+	double* grad_se;         // adjoint: per pixel d(SE count)/d theta [n_pix][6] (null: off)
+	double* grad_bse;
+	int32_t nx, ny;          // pixel grid
+	int32_t n_bins;
+	float hist_emax;
+};
+
+struct StepParams {
+	DevGeometry geom;
+	const DevMaterial* mats;
+	int32_t n_mat;
+	float energy_threshold;
+	PhiloxKey key;
+	Queue q[2][N_QUEUES];
+	uint32_t qcap;            // queue capacity = population bound (2 x capacity)
+	uint32_t capacity;        // refill target: active electrons per iteration
+	uint32_t* ctrl;           // 3 slots x SLOT_WORDS
+	const Record36* primaries;
+	uint32_t n_primaries;
+	Record36* detected;
+	uint32_t* n_detected;
+	uint32_t det_cap;
+	Tallies tal;
+	unsigned long long* counters;
+	uint32_t max_events;      // per-electron event budget
+	int32_t adjoint;          // accumulate score functions
+};
+
+// launchers
+cudaError_t launch_ray_query(const DevGeometry& g, const float* pos, const float* dir, const float* dist,
+	const int32_t* ignore_tri, const int32_t* ignore_mat, int64_t n, float* out_dist, int32_t* out_tri,
+	cudaStream_t s);
+cudaError_t launch_table_kat(const DevMaterial* mat, int which, int rounddown, int64_t n,
+	const float* x, const float* y, const float* z, float* out, cudaStream_t s);
+cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, int kind, int64_t n,
+	const float* state_in, const int32_t* mat_in, const int32_t* tri, const float* uniforms, int32_t n_uniforms,
+	float* state_out, int32_t* mat_out, int32_t* status, float* se_out, int32_t* has_se, int32_t* used,
+	cudaStream_t s);
+cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s);
+int step_grid_size(int device, int block);
+
+}  // namespace nbl

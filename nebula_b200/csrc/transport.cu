@@ -1,0 +1,468 @@
+// Electron-transport kernels for sm_100a.
+//
+// The plain method is a wavefront: every iteration is ONE launch of k_step,
+// which walks a combined index space
+//
+//     [ boundary | elastic | inelastic | new secondaries | new primaries ]
+//
+// where the first four segments are this iteration's event queues and the
+// last is the refill from the device-resident primary buffer (filled so that
+// at most `capacity` electrons are in flight).  Each item performs the
+// interaction that ended its previous free flight, then its next free flight
+// (free-path sampling + octree walk), and is appended to the next
+// iteration's queue for the event that flight ended in.  Queues are
+// structure-of-arrays and double-buffered; appends are warp-aggregated
+// (one ballot and one atomic per warp and queue), so each queue segment a
+// warp reads or writes is contiguous and coalesced.  Sorting items by event
+// kind this way replaces the reference's per-iteration radix sort of the
+// whole pool (drivers/gpu/gpu_particle_manager.inl:237-246) and keeps the
+// interaction code of a warp uniform (all lanes in one segment).
+//
+// The reference kernels this replaces: kernels::init / intersect / elastic /
+// inelastic and the pool management (drivers/gpu/gpu_driver.inl:403-566,
+// gpu_particle_manager.inl:354-376).  The per-iteration control words live
+// in three rotating slots so a kernel can read its counts, append to the next
+// slot and clear the one after without any host round trip; a run is a
+// sequence of iterations captured in CUDA graphs.
+#include "kernels.cuh"
+#include "device/rng.cuh"
+#include "device/geometry.cuh"
+#include "device/tables.cuh"
+#include "device/physics.cuh"
+
+namespace nbl {
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+	unsigned m;
+	asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+	return m;
+}
+
+// Reserve one slot per lane with `pred` from `counter`; all 32 lanes must
+// call.  Returns the lane's slot (undefined where pred is false).
+__device__ __forceinline__ uint32_t warp_reserve(uint32_t* counter, bool pred)
+{
+	const unsigned mask = __ballot_sync(0xffffffffu, pred);
+	uint32_t base = 0;
+	if (mask) {
+		const int leader = __ffs(mask) - 1;
+		if ((int)(threadIdx.x & 31) == leader)
+			base = atomicAdd(counter, (uint32_t)__popc(mask));
+		base = __shfl_sync(0xffffffffu, base, leader);
+	}
+	return base + (uint32_t)__popc(mask & lanemask_lt());
+}
+
+/* --------------------------------------------------------------- ray query */
+__global__ void k_ray_query(const DevGeometry g, const float* __restrict__ pos, const float* __restrict__ dir,
+	const float* __restrict__ dist, const int32_t* __restrict__ ignore_tri, const int32_t* __restrict__ ignore_mat,
+	int64_t n, float* __restrict__ out_dist, int32_t* __restrict__ out_tri)
+{
+	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	float d;
+	const int t = propagate(g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], dir[3 * i], dir[3 * i + 1], dir[3 * i + 2],
+		dist[i], ignore_tri[i], ignore_mat[i], d);
+	out_dist[i] = d;
+	out_tri[i] = t;
+}
+
+cudaError_t launch_ray_query(const DevGeometry& g, const float* pos, const float* dir, const float* dist,
+	const int32_t* ignore_tri, const int32_t* ignore_mat, int64_t n, float* out_dist, int32_t* out_tri,
+	cudaStream_t s)
+{
+	if (n <= 0)
+		return cudaSuccess;
+	const int block = 128;
+	const int64_t grid = (n + block - 1) / block;
+	k_ray_query<<<(unsigned)grid, block, 0, s>>>(g, pos, dir, dist, ignore_tri, ignore_mat, n, out_dist, out_tri);
+	return cudaGetLastError();
+}
+
+/* --------------------------------------------------------- table lookups */
+__global__ void k_table_kat(const DevMaterial* __restrict__ mat, int which, int rounddown, int64_t n,
+	const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z, float* __restrict__ out)
+{
+	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const DevMaterial& m = *mat;
+	float v;
+	switch (which) {
+	case 0: v = table1_get(m.el_imfp, x[i]); break;
+	case 2: v = table1_get(m.in_imfp, x[i]); break;
+	case 1: v = rounddown ? table2_rounddown(m.el_icdf, x[i], y[i]) : table2_get(m.el_icdf, x[i], y[i]); break;
+	case 3: v = rounddown ? table2_rounddown(m.in_omega, x[i], y[i]) : table2_get(m.in_omega, x[i], y[i]); break;
+	case 4: v = rounddown ? table3_rounddown(m.in_q, x[i], y[i], z[i]) : table3_get(m.in_q, x[i], y[i], z[i]); break;
+	default: v = rounddown ? table3_rounddown(m.in_binding, x[i], y[i], z[i]) : table3_get(m.in_binding, x[i], y[i], z[i]); break;
+	}
+	out[i] = v;
+}
+
+cudaError_t launch_table_kat(const DevMaterial* mat, int which, int rounddown, int64_t n,
+	const float* x, const float* y, const float* z, float* out, cudaStream_t s)
+{
+	if (n <= 0)
+		return cudaSuccess;
+	k_table_kat<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(mat, which, rounddown, n, x, y, z, out);
+	return cudaGetLastError();
+}
+
+/* ---------------------------------------------------------- single events */
+__global__ void k_event_kat(const DevGeometry g, const DevMaterial* __restrict__ mats, int kind, int64_t n,
+	const float* __restrict__ state_in, const int32_t* __restrict__ mat_in, const int32_t* __restrict__ tri,
+	const float* __restrict__ uniforms, int32_t n_uniforms, float* __restrict__ state_out,
+	int32_t* __restrict__ mat_out, int32_t* __restrict__ status, float* __restrict__ se_out,
+	int32_t* __restrict__ has_se, int32_t* __restrict__ used)
+{
+	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	ListStream rng{ uniforms + i * n_uniforms, 0u, (uint32_t)n_uniforms };
+	Electron p;
+	const float* s = state_in + 7 * i;
+	p.pos = v3(s[0], s[1], s[2]);
+	p.dir = v3(s[3], s[4], s[5]);
+	p.E = s[6];
+	int mat = mat_in[i];
+	int st = ST_RUNNING;
+	bool spawned = false;
+	Electron se;
+	se.pos = v3(0, 0, 0); se.dir = v3(0, 0, 0); se.E = 0;
+	if (kind == 3) {
+		const DevTriangle T = load_tri(g.tris, tri[i]);
+		st = boundary_event(T, mats, p, mat, rng);
+	} else if (kind == 1) {
+		spawned = inelastic_event(mats[mat], p, se, rng);
+	} else {
+		elastic_event(mats[mat], p, rng);
+	}
+	float* o = state_out + 7 * i;
+	o[0] = p.pos.x; o[1] = p.pos.y; o[2] = p.pos.z; o[3] = p.dir.x; o[4] = p.dir.y; o[5] = p.dir.z; o[6] = p.E;
+	float* so = se_out + 7 * i;
+	so[0] = se.pos.x; so[1] = se.pos.y; so[2] = se.pos.z; so[3] = se.dir.x; so[4] = se.dir.y; so[5] = se.dir.z; so[6] = se.E;
+	mat_out[i] = mat;
+	status[i] = st;
+	has_se[i] = spawned ? 1 : 0;
+	used[i] = (int32_t)rng.n;
+}
+
+cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, int kind, int64_t n,
+	const float* state_in, const int32_t* mat_in, const int32_t* tri, const float* uniforms, int32_t n_uniforms,
+	float* state_out, int32_t* mat_out, int32_t* status, float* se_out, int32_t* has_se, int32_t* used,
+	cudaStream_t s)
+{
+	if (n <= 0)
+		return cudaSuccess;
+	k_event_kat<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(g, mats, kind, n, state_in, mat_in, tri, uniforms,
+		n_uniforms, state_out, mat_out, status, se_out, has_se, used);
+	return cudaGetLastError();
+}
+
+/* ----------------------------------------------------------- transport */
+struct LocalCounters {
+	uint32_t flights, boundary, elastic, inelastic, spawned, detected, terminated, primaries;
+	uint32_t walk_overflow, nan, queue_overflow, record_overflow, budget, deferred;
+};
+
+// Free flight(s) from the electron's current state: domain and energy cut,
+// free-path sampling, octree walk, move.  Flights in vacuum that hit nothing
+// end without an event and are repeated (the next one leaves the domain).
+// Returns the queue of the event the flight ends in, or -1 when the electron
+// is terminated.  Mirrors cpu_driver::init / kernels::init
+// (drivers/cpu/cpu_driver.inl:74-130, drivers/gpu/gpu_driver.inl:403-480).
+template<bool ADJ>
+__device__ __forceinline__ int free_flight(const StepParams& P, Electron& p, int mat, int& last_tri, uint32_t& event,
+	uint32_t tag, uint64_t lineage, float* sc, LocalCounters& lc)
+{
+	for (int hop = 0; hop < 4; ++hop) {
+		++lc.flights;
+		if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) { ++lc.nan; return -1; }
+		if (!in_domain(P.geom, p.pos.x, p.pos.y, p.pos.z))
+			return -1;
+		if (event >= P.max_events) { ++lc.budget; return -1; }
+		++event;
+		int type = 0;
+		float dist = P.geom.max_extent;
+		float mu_el = 0.0f, mu_in = 0.0f;
+		const DevMaterial* m = nullptr;
+		if (mat >= 0) {
+			m = P.mats + mat;
+			if (p.E < fa(m->barrier, P.energy_threshold))
+				return -1;
+			PhiloxStream r;
+			r.init(P.key, event, 0u, tag, lineage);
+			const float pe = sample_path(m->el_imfp, m->el_scale, p.E, r, mu_el);
+			const float pi = sample_path(m->in_imfp, m->in_scale, p.E, r, mu_in);
+			dist = __int_as_float(0x7f800000);
+			if (pe < dist) { dist = pe; type = 2; }
+			if (pi < dist) { dist = pi; type = 1; }
+		}
+		const V3 d = vnormalised(p.dir);
+		float idist;
+		const int hit = propagate(P.geom, p.pos.x, p.pos.y, p.pos.z, d.x, d.y, d.z, dist, last_tri, mat, idist);
+		if (hit == -2) { ++lc.walk_overflow; return -1; }
+		if (ADJ && mat >= 0 && mat < 2) {
+			// score of the flight: density mu_k exp(-(mu_in+mu_el) d) of the
+			// chosen event k at distance d, or survival exp(-(mu_in+mu_el) d)
+			// when a boundary cuts the flight; derivative w.r.t. the scales
+			const float travel = hit >= 0 ? idist : dist;
+			const float in_k = (hit < 0 && type == 1) ? 1.0f : 0.0f;
+			const float el_k = (hit < 0 && type == 2) ? 1.0f : 0.0f;
+			sc[3 * mat + 0] += (in_k - mu_in * travel) / m->in_scale;
+			sc[3 * mat + 1] += (el_k - mu_el * travel) / m->el_scale;
+		}
+		if (hit >= 0) {
+			p.pos = vadd(p.pos, vmul(d, idist));
+			last_tri = hit;
+			return EV_BOUNDARY;
+		}
+		p.pos = vadd(p.pos, vmul(d, dist));
+		if (type == 1) return EV_INELASTIC;
+		if (type == 2) return EV_ELASTIC;
+	}
+	return -1;
+}
+
+__device__ __forceinline__ void store_electron(const Queue& q, uint32_t slot, const Electron& p, int mat, int last_tri,
+	uint32_t tag, uint32_t event, uint64_t lineage)
+{
+	q.a[slot] = make_float4(p.pos.x, p.pos.y, p.pos.z, p.E);
+	q.b[slot] = make_float4(p.dir.x, p.dir.y, p.dir.z, __int_as_float(mat));
+	q.c[slot] = make_uint4((uint32_t)last_tri, tag, event, (uint32_t)lineage);
+	q.d[slot] = (uint32_t)(lineage >> 32);
+}
+
+template<bool ADJ>
+__global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
+{
+	const uint32_t rs = it % 3u, ws = (it + 1u) % 3u, zs = (it + 2u) % 3u;
+	const uint32_t* cr = P.ctrl + rs * SLOT_WORDS;
+	uint32_t* cw = P.ctrl + ws * SLOT_WORDS;
+	// counts are clamped to the queue capacity (the secondary budget below
+	// keeps them there; the clamp makes an out-of-range read impossible)
+	const uint32_t n0 = min(cr[0], P.qcap), n1 = min(cr[1], P.qcap), n2 = min(cr[2], P.qcap), n3 = min(cr[3], P.qcap);
+	const uint32_t cursor = cr[SLOT_CURSOR];
+	const uint32_t e1 = n0 + n1, e2 = e1 + n2, active = e2 + n3;
+	const uint32_t room = active < P.capacity ? P.capacity - active : 0u;
+	const uint32_t left = P.n_primaries - cursor;
+	const uint32_t nr = room < left ? room : left;
+	const uint32_t total = active + nr;
+	// Secondary budget: every item leaves at most one electron in the next
+	// queues plus at most one secondary, so allowing at most qcap - total
+	// secondaries keeps next iteration's population, and hence every queue,
+	// within qcap.  An inelastic event that finds the budget spent is deferred
+	// unchanged to the next iteration (the reference's PENDING state,
+	// drivers/gpu/gpu_driver.inl:522-527); its random stream is keyed by its
+	// event counter, so deferral does not change its outcome.
+	const uint32_t se_budget = P.qcap > total ? P.qcap - total : 0u;
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		cw[SLOT_CURSOR] = cursor + nr;
+		uint32_t* cz = P.ctrl + zs * SLOT_WORDS;
+#pragma unroll
+		for (int k = 0; k < SLOT_WORDS; ++k)
+			cz[k] = 0u;
+	}
+	const Queue* qin = P.q[it & 1u];
+	const Queue* qout = P.q[(it + 1u) & 1u];
+
+	LocalCounters lc = {};
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+
+	for (uint32_t base = warp * 32u; base < total; base += n_warps * 32u) {
+		const uint32_t item = base + lane;
+		int kind = -1;
+		uint32_t qi = 0;
+		if (item < total) {
+			if (item < n0) { kind = EV_BOUNDARY; qi = item; }
+			else if (item < e1) { kind = EV_ELASTIC; qi = item - n0; }
+			else if (item < e2) { kind = EV_INELASTIC; qi = item - e1; }
+			else if (item < active) { kind = EV_NEW; qi = item - e2; }
+			else { kind = 4; qi = cursor + (item - active); }
+		}
+
+		Electron p;
+		int mat = MAT_VACUUM, last_tri = -1;
+		uint32_t tag = 0, event = 0;
+		uint64_t lineage = 0;
+		float sc[6];
+#pragma unroll
+		for (int k = 0; k < 6; ++k) sc[k] = 0.0f;
+		if (kind >= 0 && kind < 4) {
+			const Queue& q = qin[kind];
+			const float4 a = q.a[qi], b = q.b[qi];
+			const uint4 c = q.c[qi];
+			p.pos = v3(a.x, a.y, a.z); p.E = a.w;
+			p.dir = v3(b.x, b.y, b.z); mat = __float_as_int(b.w);
+			last_tri = (int)c.x; tag = c.y; event = c.z;
+			lineage = ((uint64_t)q.d[qi] << 32) | c.w;
+			if (ADJ) {
+				const float4 s = q.s[qi];
+				const float2 s2 = q.s2[qi];
+				sc[0] = s.x; sc[1] = s.y; sc[2] = s.z; sc[3] = s.w; sc[4] = s2.x; sc[5] = s2.y;
+			}
+		} else if (kind == 4) {
+			const Record36* r = P.primaries + qi;
+			p.pos = v3(r->x, r->y, r->z);
+			p.dir = v3(r->dx, r->dy, r->dz);
+			p.E = r->E;
+			tag = qi;
+			++lc.primaries;
+		}
+
+		// interaction that ended the previous flight
+		int status = (kind >= 0) ? ST_RUNNING : ST_TERMINATED;
+		bool spawn = false;
+		Electron se;
+		const uint32_t ticket = warp_reserve(cw + SLOT_TICKETS, kind == EV_INELASTIC);
+		const bool deferred = kind == EV_INELASTIC && ticket >= se_budget;
+		if (deferred) {
+			++lc.deferred;
+		} else if (kind == EV_BOUNDARY) {
+			++lc.boundary;
+			PhiloxStream r;
+			r.init(P.key, event, 1u, tag, lineage);
+			const DevTriangle T = load_tri(P.geom.tris, last_tri);
+			if (ADJ) {
+				BoundaryScore bs = { 0.0f, 0.0f, -1, -1 };
+				status = boundary_event(T, P.mats, p, mat, r, &bs);
+				// the work function enters through barrier = fermi + W of the
+				// materials on either side of the crossing
+				if (bs.mat_in >= 0 && bs.mat_in < 2) sc[3 * bs.mat_in + 2] += bs.d_in;
+				if (bs.mat_out >= 0 && bs.mat_out < 2) sc[3 * bs.mat_out + 2] += bs.d_out;
+			} else {
+				status = boundary_event(T, P.mats, p, mat, r);
+			}
+		} else if (kind == EV_ELASTIC) {
+			++lc.elastic;
+			last_tri = -1;
+			PhiloxStream r;
+			r.init(P.key, event, 1u, tag, lineage);
+			elastic_event(P.mats[mat], p, r);
+		} else if (kind == EV_INELASTIC) {
+			++lc.inelastic;
+			last_tri = -1;
+			PhiloxStream r;
+			r.init(P.key, event, 1u, tag, lineage);
+			spawn = inelastic_event(P.mats[mat], p, se, r);
+		}
+
+		// detection output: record + tallies
+		if (status == ST_DETECTED) {
+			++lc.detected;
+			const Record36* pr = P.primaries + tag;
+			const int px = pr->px, py = pr->py;
+			const Tallies& T = P.tal;
+			if (T.se_img && px >= 0 && py >= 0 && px < T.nx && py < T.ny) {
+				const size_t pix = (size_t)py * T.nx + px;
+				atomicAdd((p.E < 50.0f ? T.se_img : T.bse_img) + pix, 1u);
+				if (ADJ && T.grad_se) {
+					double* g = (p.E < 50.0f ? T.grad_se : T.grad_bse) + pix * 6;
+#pragma unroll
+					for (int k = 0; k < 6; ++k)
+						atomicAdd(g + k, (double)sc[k]);
+				}
+			}
+			if (T.hist && p.E >= 0.0f && p.E < T.hist_emax) {
+				int bin = (int)(p.E / T.hist_emax * (float)T.n_bins);
+				bin = bin < T.n_bins ? bin : T.n_bins - 1;
+				atomicAdd(T.hist + bin, 1u);
+			}
+		}
+		const bool det = status == ST_DETECTED;
+		const uint32_t rslot = warp_reserve(P.n_detected, det);
+		if (det) {
+			if (rslot < P.det_cap) {
+				Record36 rec;
+				const Record36* pr = P.primaries + tag;
+				rec.x = p.pos.x; rec.y = p.pos.y; rec.z = p.pos.z;
+				rec.dx = p.dir.x; rec.dy = p.dir.y; rec.dz = p.dir.z; rec.E = p.E;
+				rec.px = pr->px; rec.py = pr->py;
+				P.detected[rslot] = rec;
+			} else {
+				++lc.record_overflow;
+			}
+		}
+
+		// secondary: inherits material, tag and the parent's scores; its
+		// lineage id is derived from the parent's and the spawning event
+		uint64_t se_lineage = 0;
+		if (spawn) {
+			++lc.spawned;
+			se_lineage = child_lineage(lineage, event);
+		}
+		const uint32_t sslot = warp_reserve(cw + EV_NEW, spawn);
+		if (spawn) {
+			if (sslot < P.qcap) {
+				store_electron(qout[EV_NEW], sslot, se, mat, -1, tag, 0u, se_lineage);
+				if (ADJ) {
+					qout[EV_NEW].s[sslot] = make_float4(sc[0], sc[1], sc[2], sc[3]);
+					qout[EV_NEW].s2[sslot] = make_float2(sc[4], sc[5]);
+				}
+			} else {
+				++lc.queue_overflow;
+			}
+		}
+
+		// next free flight (a deferred event waits in its queue instead)
+		int qtype = -1;
+		if (deferred)
+			qtype = EV_INELASTIC;
+		else if (status == ST_RUNNING)
+			qtype = free_flight<ADJ>(P, p, mat, last_tri, event, tag, lineage, sc, lc);
+		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
+			++lc.terminated;
+#pragma unroll
+		for (int t = 0; t < 3; ++t) {
+			const bool mine = qtype == t;
+			const uint32_t slot = warp_reserve(cw + t, mine);
+			if (mine) {
+				if (slot < P.qcap) {
+					store_electron(qout[t], slot, p, mat, last_tri, tag, event, lineage);
+					if (ADJ) {
+						qout[t].s[slot] = make_float4(sc[0], sc[1], sc[2], sc[3]);
+						qout[t].s2[slot] = make_float2(sc[4], sc[5]);
+					}
+				} else {
+					++lc.queue_overflow;
+				}
+			}
+		}
+	}
+
+	// flush counters: one atomic per warp and counter
+	const uint32_t vals[N_COUNTERS] = { lc.flights, lc.boundary, lc.elastic, lc.inelastic, lc.spawned,
+		lc.detected, lc.terminated, lc.primaries, lc.walk_overflow, lc.nan, lc.queue_overflow,
+		lc.record_overflow, lc.budget, lc.deferred };
+#pragma unroll
+	for (int k = 0; k < N_COUNTERS; ++k) {
+		const uint32_t v = __reduce_add_sync(0xffffffffu, vals[k]);
+		if (lane == 0 && v)
+			atomicAdd(P.counters + k, (unsigned long long)v);
+	}
+}
+
+cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)
+{
+	if (p.adjoint)
+		k_step<true><<<grid, block, 0, s>>>(p, iteration);
+	else
+		k_step<false><<<grid, block, 0, s>>>(p, iteration);
+	return cudaGetLastError();
+}
+
+int step_grid_size(int device, int block)
+{
+	int sms = 148, per_sm = 1;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<false>, block, 0);
+	if (per_sm < 1)
+		per_sm = 1;
+	return sms * per_sm;
+}
+
+}  // namespace nbl
