@@ -174,7 +174,8 @@ void nbl_physics_defaults(nbl_physics_opts* o);
 /* ------------------------------------------------------------ simulation */
 typedef struct nbl_params {
 	int32_t device;              /* CUDA device ordinal */
-	uint32_t capacity;           /* electrons in flight (refill target); 0: 1 << 20 */
+	uint32_t capacity;           /* refill target: primaries are added while fewer electrons are in
+	                                flight; queues hold up to 8x this (secondaries); 0: 1 << 20 */
 	float energy_threshold;      /* eV above the vacuum level, gpu_driver.h:56-59 */
 	uint64_t seed;
 	uint32_t block_size;         /* 0: 256 */
@@ -198,7 +199,7 @@ typedef struct nbl_counters {
 	uint64_t boundary, elastic, inelastic;
 	uint64_t spawned, detected, terminated, primaries_started;
 	uint64_t walk_overflow, nan_state, queue_overflow, record_overflow, event_budget;
-	uint64_t deferred;           /* inelastic events postponed for lack of secondary room */
+	uint64_t spilled;            /* secondaries parked in the overflow ring for lack of queue room */
 	uint64_t iterations;         /* wavefront iterations launched */
 	uint64_t primaries_total;    /* primaries pushed */
 	uint64_t records_pending;    /* detected records not yet drained */

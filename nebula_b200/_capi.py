@@ -70,7 +70,7 @@ class Params(C.Structure):
 
 COUNTER_NAMES = ("flights", "boundary", "elastic", "inelastic", "spawned", "detected", "terminated",
                  "primaries_started", "walk_overflow", "nan_state", "queue_overflow",
-                 "record_overflow", "event_budget", "deferred", "iterations", "primaries_total",
+                 "record_overflow", "event_budget", "spilled", "iterations", "primaries_total",
                  "records_pending")
 
 

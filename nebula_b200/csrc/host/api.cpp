@@ -187,6 +187,7 @@ struct nbl_sim {
 	DeviceGeometry geom;
 	DeviceMaterials mats;
 	DevBuf queues[2][N_QUEUES][6];
+	DevBuf spill[6];
 	DevBuf ctrl, counters, detected, n_detected, se_img, bse_img, hist, grad_se, grad_bse;
 	DevBuf primaries;
 	uint64_t pri_cap = 0, n_pri = 0;
@@ -273,19 +274,43 @@ struct nbl_sim {
 	int64_t advance(uint64_t max_graphs)
 	{
 		uint32_t c[SLOT_WORDS + 1];
+		uint64_t stalled = 0, last_progress = ~0ull;
 		for (uint64_t k = 0; k < max_graphs; ++k) {
 			launch_graph();
 			read_ctrl(c);
 			const uint32_t ndet = pinned_ctrl[SLOT_WORDS];
 			if (ndet > sp.det_cap / 4)
 				drain_to_host(ndet);
-			const uint64_t active = (uint64_t)c[0] + c[1] + c[2] + c[3];
+			const uint64_t active = (uint64_t)c[0] + c[1] + c[2] + c[3] + spill_occupancy(c);
 			const uint64_t left = n_pri - c[SLOT_CURSOR];
 			if (active == 0 && left == 0)
 				return 0;
+			// every iteration with work makes flights; none for two whole
+			// graphs means the run cannot progress: report it, never spin
+			const uint64_t progress = flights_done();
+			if (progress == last_progress) {
+				if (++stalled >= 2)
+					throw Error(NBL_ERR_POOL_OVERFLOW, "no electron moved for two graphs of iterations");
+			} else {
+				stalled = 0;
+			}
+			last_progress = progress;
 		}
 		read_ctrl(c);
-		return (int64_t)((uint64_t)c[0] + c[1] + c[2] + c[3] + (n_pri - c[SLOT_CURSOR]));
+		return (int64_t)((uint64_t)c[0] + c[1] + c[2] + c[3] + spill_occupancy(c) + (n_pri - c[SLOT_CURSOR]));
+	}
+
+	static uint32_t spill_occupancy(const uint32_t* c)
+	{
+		return c[SLOT_SPILL_TAIL] + c[SLOT_SPILL_PUSHED] - c[SLOT_SPILL_HEAD];
+	}
+
+	uint64_t flights_done()
+	{
+		unsigned long long f = 0;
+		CU(cudaMemcpyAsync(&f, counters.as<unsigned long long>() + CNT_FLIGHTS, sizeof(f), cudaMemcpyDeviceToHost, stream));
+		CU(cudaStreamSynchronize(stream));
+		return f;
 	}
 
 	void check_errors()
@@ -294,7 +319,7 @@ struct nbl_sim {
 		CU(cudaMemcpyAsync(cnt, counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
 		CU(cudaStreamSynchronize(stream));
 		if (cnt[CNT_QUEUE_OVERFLOW] || cnt[CNT_RECORD_OVERFLOW])
-			throw Error(NBL_ERR_POOL_OVERFLOW, "event queue or record buffer overflowed (" +
+			throw Error(NBL_ERR_POOL_OVERFLOW, "secondary overflow ring or record buffer full (" +
 				std::to_string(cnt[CNT_QUEUE_OVERFLOW]) + " electrons, " + std::to_string(cnt[CNT_RECORD_OVERFLOW]) +
 				" records dropped); raise capacity / record_capacity");
 		if (cnt[CNT_NAN])
@@ -663,7 +688,14 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		sp.key.k0 = (uint32_t)params->seed;
 		sp.key.k1 = (uint32_t)(params->seed >> 32);
 		sp.capacity = cap;
-		sp.qcap = 2 * cap;
+		// population bound: a cascade grows the population well past the
+		// number of primaries refilled, so every queue is sized for 8x the
+		// refill target; the secondary budget keeps the population below it
+		require((uint64_t)cap * 8 < (1ull << 30), "capacity too large");
+		sp.qcap = 8 * cap;
+		// refill at most 1/16 of the target per iteration, so the population
+		// ramps up while the cascades of the first primaries develop
+		sp.ramp = std::max<uint32_t>(cap / 16, 256);
 		const bool adj = params->adjoint != 0;
 		for (int b = 0; b < 2; ++b)
 			for (int q = 0; q < N_QUEUES; ++q) {
@@ -680,6 +712,24 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 				Q.a = qb[0].as<float4>(); Q.b = qb[1].as<float4>(); Q.c = qb[2].as<uint4>(); Q.d = qb[3].as<uint32_t>();
 				Q.s = qb[4].as<float4>(); Q.s2 = qb[5].as<float2>();
 			}
+		{
+			// overflow ring: at least twice the population bound, >= 2^20
+			uint32_t ring = 1u << 20;
+			while (ring < 2 * sp.qcap) ring <<= 1;
+			DevBuf* qb = s->spill;
+			qb[0].alloc((size_t)ring * sizeof(float4));
+			qb[1].alloc((size_t)ring * sizeof(float4));
+			qb[2].alloc((size_t)ring * sizeof(uint4));
+			qb[3].alloc((size_t)ring * sizeof(uint32_t));
+			if (adj) {
+				qb[4].alloc((size_t)ring * sizeof(float4));
+				qb[5].alloc((size_t)ring * sizeof(float2));
+			}
+			Queue& Q = sp.spill;
+			Q.a = qb[0].as<float4>(); Q.b = qb[1].as<float4>(); Q.c = qb[2].as<uint4>(); Q.d = qb[3].as<uint32_t>();
+			Q.s = qb[4].as<float4>(); Q.s2 = qb[5].as<float2>();
+			sp.spill_mask = ring - 1;
+		}
 		s->ctrl.alloc(3 * SLOT_WORDS * sizeof(uint32_t));
 		sp.ctrl = s->ctrl.as<uint32_t>();
 		s->counters.alloc(N_COUNTERS * sizeof(unsigned long long));
@@ -839,7 +889,7 @@ nbl_status nbl_sim_counters(nbl_sim* s, nbl_counters* out)
 		out->walk_overflow = c[CNT_WALK_OVERFLOW]; out->nan_state = c[CNT_NAN];
 		out->queue_overflow = c[CNT_QUEUE_OVERFLOW]; out->record_overflow = c[CNT_RECORD_OVERFLOW];
 		out->event_budget = c[CNT_EVENT_BUDGET];
-		out->deferred = c[CNT_DEFERRED];
+		out->spilled = c[CNT_SPILLED];
 		out->iterations = s->iteration;
 		out->primaries_total = s->n_pri;
 		out->records_pending = s->host_records.size() + std::min(d, s->sp.det_cap);

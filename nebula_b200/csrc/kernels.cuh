@@ -23,14 +23,18 @@ struct Queue {
 enum : int {
 	CNT_FLIGHTS = 0, CNT_BOUNDARY, CNT_ELASTIC, CNT_INELASTIC, CNT_SPAWNED, CNT_DETECTED,
 	CNT_TERMINATED, CNT_PRIMARIES, CNT_WALK_OVERFLOW, CNT_NAN, CNT_QUEUE_OVERFLOW,
-	CNT_RECORD_OVERFLOW, CNT_EVENT_BUDGET, CNT_DEFERRED, N_COUNTERS
+	CNT_RECORD_OVERFLOW, CNT_EVENT_BUDGET, CNT_SPILLED, N_COUNTERS
 };
 
-// Per-iteration control words, three rotating slots of 8 words:
-// [queue counts x4, primary cursor, secondary tickets, pad x2].
-constexpr int SLOT_WORDS = 8;
+// Per-iteration control words, three rotating slots of 16 words:
+// [queue counts x4, primary cursor, secondary tickets, spill head, spill tail
+//  at iteration start, spill pushes this iteration, pad].
+constexpr int SLOT_WORDS = 16;
 constexpr int SLOT_CURSOR = 4;
 constexpr int SLOT_TICKETS = 5;
+constexpr int SLOT_SPILL_HEAD = 6;
+constexpr int SLOT_SPILL_TAIL = 7;
+constexpr int SLOT_SPILL_PUSHED = 8;
 
 struct Tallies {
 	uint32_t* se_img;        // per pixel counts of detected E < 50 eV (null: off)
@@ -50,8 +54,11 @@ struct StepParams {
 	float energy_threshold;
 	PhiloxKey key;
 	Queue q[2][N_QUEUES];
-	uint32_t qcap;            // queue capacity = population bound (2 x capacity)
+	uint32_t qcap;            // queue capacity = population bound
 	uint32_t capacity;        // refill target: active electrons per iteration
+	uint32_t ramp;            // most primaries refilled per iteration
+	Queue spill;              // ring of secondaries that did not fit (power-of-two size)
+	uint32_t spill_mask;      // ring size - 1
 	uint32_t* ctrl;           // 3 slots x SLOT_WORDS
 	const Record36* primaries;
 	uint32_t n_primaries;

@@ -7,7 +7,7 @@
 //
 // where the first four segments are this iteration's event queues and the
 // last is the refill from the device-resident primary buffer (filled so that
-// at most `capacity` electrons are in flight).  Each item performs the
+// at most `capacity` electrons are in flight, at most `ramp` per iteration).  Each item performs the
 // interaction that ended its previous free flight, then its next free flight
 // (free-path sampling + octree walk), and is appended to the next
 // iteration's queue for the event that flight ended in.  Queues are
@@ -164,7 +164,7 @@ cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, int 
 /* ----------------------------------------------------------- transport */
 struct LocalCounters {
 	uint32_t flights, boundary, elastic, inelastic, spawned, detected, terminated, primaries;
-	uint32_t walk_overflow, nan, queue_overflow, record_overflow, budget, deferred;
+	uint32_t walk_overflow, nan, queue_overflow, record_overflow, budget, spilled;
 };
 
 // Free flight(s) from the electron's current state: domain and energy cut,
@@ -246,20 +246,30 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 	const uint32_t n0 = min(cr[0], P.qcap), n1 = min(cr[1], P.qcap), n2 = min(cr[2], P.qcap), n3 = min(cr[3], P.qcap);
 	const uint32_t cursor = cr[SLOT_CURSOR];
 	const uint32_t e1 = n0 + n1, e2 = e1 + n2, active = e2 + n3;
-	const uint32_t room = active < P.capacity ? P.capacity - active : 0u;
+	// spill ring: secondaries that found no room earlier, drained (oldest
+	// first) ahead of new primaries while the population has room
+	const uint32_t sp_head = cr[SLOT_SPILL_HEAD];
+	const uint32_t sp_tail = cr[SLOT_SPILL_TAIL] + cr[SLOT_SPILL_PUSHED];
+	const uint32_t sp_room = active < P.qcap ? P.qcap - active : 0u;
+	const uint32_t n_drain = min(sp_tail - sp_head, sp_room);
+	const uint32_t e3 = active + n_drain;
+	// no new primaries while secondaries are still parked in the ring
+	const bool parked = sp_tail - sp_head > n_drain;
+	const uint32_t room = (e3 < P.capacity && !parked) ? P.capacity - e3 : 0u;
 	const uint32_t left = P.n_primaries - cursor;
-	const uint32_t nr = room < left ? room : left;
-	const uint32_t total = active + nr;
+	const uint32_t nr = min(min(room, left), P.ramp);
+	const uint32_t total = e3 + nr;
 	// Secondary budget: every item leaves at most one electron in the next
-	// queues plus at most one secondary, so allowing at most qcap - total
-	// secondaries keeps next iteration's population, and hence every queue,
-	// within qcap.  An inelastic event that finds the budget spent is deferred
-	// unchanged to the next iteration (the reference's PENDING state,
-	// drivers/gpu/gpu_driver.inl:522-527); its random stream is keyed by its
-	// event counter, so deferral does not change its outcome.
+	// queues plus at most one secondary, so queueing at most qcap - total
+	// secondaries keeps the next population, and hence every queue, within
+	// qcap.  Secondaries beyond the budget go to the spill ring (the
+	// reference instead holds the parent back, PENDING in
+	// drivers/gpu/gpu_driver.inl:522-527, which can deadlock a full pool).
 	const uint32_t se_budget = P.qcap > total ? P.qcap - total : 0u;
 	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		cw[SLOT_CURSOR] = cursor + nr;
+		cw[SLOT_SPILL_HEAD] = sp_head + n_drain;
+		cw[SLOT_SPILL_TAIL] = sp_tail;
 		uint32_t* cz = P.ctrl + zs * SLOT_WORDS;
 #pragma unroll
 		for (int k = 0; k < SLOT_WORDS; ++k)
@@ -282,7 +292,8 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 			else if (item < e1) { kind = EV_ELASTIC; qi = item - n0; }
 			else if (item < e2) { kind = EV_INELASTIC; qi = item - e1; }
 			else if (item < active) { kind = EV_NEW; qi = item - e2; }
-			else { kind = 4; qi = cursor + (item - active); }
+			else if (item < e3) { kind = 5; qi = (sp_head + (item - active)) & P.spill_mask; }
+			else { kind = 4; qi = cursor + (item - e3); }
 		}
 
 		Electron p;
@@ -292,8 +303,8 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 		float sc[6];
 #pragma unroll
 		for (int k = 0; k < 6; ++k) sc[k] = 0.0f;
-		if (kind >= 0 && kind < 4) {
-			const Queue& q = qin[kind];
+		if (kind == 5 || (kind >= 0 && kind < 4)) {
+			const Queue& q = kind == 5 ? P.spill : qin[kind];
 			const float4 a = q.a[qi], b = q.b[qi];
 			const uint4 c = q.c[qi];
 			p.pos = v3(a.x, a.y, a.z); p.E = a.w;
@@ -318,11 +329,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 		int status = (kind >= 0) ? ST_RUNNING : ST_TERMINATED;
 		bool spawn = false;
 		Electron se;
-		const uint32_t ticket = warp_reserve(cw + SLOT_TICKETS, kind == EV_INELASTIC);
-		const bool deferred = kind == EV_INELASTIC && ticket >= se_budget;
-		if (deferred) {
-			++lc.deferred;
-		} else if (kind == EV_BOUNDARY) {
+		if (kind == EV_BOUNDARY) {
 			++lc.boundary;
 			PhiloxStream r;
 			r.init(P.key, event, 1u, tag, lineage);
@@ -395,24 +402,36 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 			++lc.spawned;
 			se_lineage = child_lineage(lineage, event);
 		}
-		const uint32_t sslot = warp_reserve(cw + EV_NEW, spawn);
-		if (spawn) {
-			if (sslot < P.qcap) {
-				store_electron(qout[EV_NEW], sslot, se, mat, -1, tag, 0u, se_lineage);
-				if (ADJ) {
-					qout[EV_NEW].s[sslot] = make_float4(sc[0], sc[1], sc[2], sc[3]);
-					qout[EV_NEW].s2[sslot] = make_float2(sc[4], sc[5]);
-				}
+		const uint32_t ticket = warp_reserve(cw + SLOT_TICKETS, spawn);
+		const bool queued = spawn && ticket < se_budget;
+		const bool spilled = spawn && !queued;
+		const uint32_t sslot = warp_reserve(cw + EV_NEW, queued);
+		const uint32_t pslot = warp_reserve(cw + SLOT_SPILL_PUSHED, spilled);
+		if (queued || spilled) {
+			const Queue* dst = nullptr;
+			uint32_t at = 0;
+			if (queued) {
+				if (sslot < P.qcap) { dst = &qout[EV_NEW]; at = sslot; }
+				else ++lc.queue_overflow;
 			} else {
-				++lc.queue_overflow;
+				++lc.spilled;
+				// the ring holds at most spill_mask + 1 electrons, counting the
+				// ones being drained during this iteration
+				if (sp_tail + pslot - sp_head <= P.spill_mask) { dst = &P.spill; at = (sp_tail + pslot) & P.spill_mask; }
+				else ++lc.queue_overflow;
+			}
+			if (dst) {
+				store_electron(*dst, at, se, mat, -1, tag, 0u, se_lineage);
+				if (ADJ) {
+					dst->s[at] = make_float4(sc[0], sc[1], sc[2], sc[3]);
+					dst->s2[at] = make_float2(sc[4], sc[5]);
+				}
 			}
 		}
 
-		// next free flight (a deferred event waits in its queue instead)
+		// next free flight
 		int qtype = -1;
-		if (deferred)
-			qtype = EV_INELASTIC;
-		else if (status == ST_RUNNING)
+		if (status == ST_RUNNING)
 			qtype = free_flight<ADJ>(P, p, mat, last_tri, event, tag, lineage, sc, lc);
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
 			++lc.terminated;
@@ -437,7 +456,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 	// flush counters: one atomic per warp and counter
 	const uint32_t vals[N_COUNTERS] = { lc.flights, lc.boundary, lc.elastic, lc.inelastic, lc.spawned,
 		lc.detected, lc.terminated, lc.primaries, lc.walk_overflow, lc.nan, lc.queue_overflow,
-		lc.record_overflow, lc.budget, lc.deferred };
+		lc.record_overflow, lc.budget, lc.spilled };
 #pragma unroll
 	for (int k = 0; k < N_COUNTERS; ++k) {
 		const uint32_t v = __reduce_add_sync(0xffffffffu, vals[k]);

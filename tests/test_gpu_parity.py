@@ -78,7 +78,11 @@ def test_table_lookup_bit_exact(inputs, which, rank):
         got = m.table_lookup(which, x, y, z, rounddown=rd)
         fn = O.lib().orc_table_rounddown if rd else O.lib().orc_table_get
         exp = np.array([fn(t, rank, float(a), float(b), float(c)) for a, b, c in zip(x, y, z)], np.float32)
-        assert np.array_equal(got.view(np.uint32), exp.view(np.uint32)), (which, rd)
+        # bit-exact, with every NaN equal to every NaN (rows below the Fermi
+        # energy hold -inf, whose interpolation gives NaN on both sides)
+        both_nan = np.isnan(got) & np.isnan(exp)
+        assert np.array_equal(np.where(both_nan, 0, got.view(np.uint32)),
+                              np.where(both_nan, 0, exp.view(np.uint32))), (which, rd)
 
 
 def _event_cases(kind, n, rng, n_tri=None):
@@ -245,13 +249,17 @@ def test_transport_deterministic_and_capacity_independent(inputs):
     m = nb.Material.load(inputs["si.nmat"])
     pri = primaries.point_beam(3000)
     outs = []
-    for cap, blk in ((1 << 12, 256), (1 << 16, 128), (300, 64)):
+    spilled = []
+    for cap, blk in ((1 << 16, 256), (1 << 12, 128), (64, 64)):
         sim = nb.Simulation(g, [m], capacity=cap, seed=42, block_size=blk)
         sim.push(pri)
         sim.run()
         r = sim.flush_detected()
-        outs.append(np.sort(r.view(np.dtype((np.void, 36)))))
+        spilled.append(sim.counters()["spilled"])
+        outs.append(np.sort(r.view(np.dtype((np.void, 36))).ravel()))
     assert outs[0].tobytes() == outs[1].tobytes() == outs[2].tobytes()
+    # the smallest pool must have parked secondaries in the overflow ring
+    assert spilled[2] > 0
 
 
 def test_small_capacity_forces_many_refills(inputs):
@@ -259,10 +267,10 @@ def test_small_capacity_forces_many_refills(inputs):
     from nebula_b200.synth import primaries
     g = nb.Geometry.from_tri_file(inputs["slab.tri"])
     m = nb.Material.load(inputs["si.nmat"])
-    pri = primaries.point_beam(200, energy=5000.0)
+    pri = primaries.point_beam(300, energy=1000.0)
     sim = nb.Simulation(g, [m], capacity=64, seed=1, iterations_per_graph=6)
     sim.push(pri)
     sim.run()
     c = sim.counters()
-    assert c["primaries_started"] == 200
+    assert c["primaries_started"] == 300
     assert c["primaries_started"] + c["spawned"] == c["detected"] + c["terminated"]
