@@ -234,6 +234,32 @@ nbl_status nbl_sim_reset(nbl_sim* s);
 nbl_status nbl_sim_kernel_ms(nbl_sim* s, double* ms);
 void nbl_sim_destroy(nbl_sim* s);
 
+/* ------------------------------------------------------------ run without allocation */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (an embedding host whose allocator owns the device, a real-time loop
+ * where an allocation could block or fail): the same transport as
+ * nbl_sim_run, with all scratch -- queues, overflow ring, control words,
+ * counters, device copies of geometry and tables -- in one fixed array of
+ * NBL_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit.  No cudaMalloc/cudaFree or other allocating call is made.
+ *   inputs : geometry and materials (host handles), primaries in device memory
+ *   outputs: detected records (device, records_cap of them) and their count,
+ *            optional per-pixel SE/BSE images (tally_nx x tally_ny, device) and
+ *            histogram (hist_bins, device), all cleared first; counters (host)
+ * Limits: capacity <= NBL_NOALLOC_MAX_CAPACITY (0 selects it), at most
+ * NBL_NOALLOC_MAX_MATERIALS materials, geometry <= 2 MiB and tables <= 4 MiB
+ * in device layout, no adjoint; larger inputs are rejected.  The first call on
+ * a device looks up the array's address; make it before any stream capture.
+ * Calls share the array and it keeps the previous call's contents: each call
+ * clears what must start at zero, and calls that overlap on the GPU race. */
+#define NBL_NOALLOC_MAX_CAPACITY 2048
+#define NBL_NOALLOC_MAX_MATERIALS 4
+#define NBL_NOALLOC_SCRATCH_BYTES 14813184
+nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
+	const nbl_params* params, const nbl_record* d_primaries, int64_t n_primaries, nbl_record* d_records,
+	int64_t records_cap, int64_t* n_records, uint32_t* d_se_img, uint32_t* d_bse_img, uint32_t* d_hist,
+	nbl_counters* counters);
+
 /* ------------------------------------------------------------ debug entry points */
 /* Table lookups on the device (which: 0 el_imfp 1 el_icdf 2 in_imfp 3 in_omega
  * 4 in_q 5 in_binding) for n points; `rounddown` selects get_rounddown. */

@@ -112,6 +112,9 @@ _DECLS = [
     ("nbl_sim_reset", C.c_int, [C.c_void_p]),
     ("nbl_sim_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_destroy", None, [C.c_void_p]),
+    ("nbl_run_noalloc", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(Params), C.c_void_p,
+                                  C.c_int64, C.c_void_p, C.c_int64, i64p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(Counters)]),
     ("nbl_debug_table_lookup", C.c_int, [C.c_void_p, C.c_int, C.c_int32, C.c_int32, C.c_int64, f32p, f32p, f32p,
                                          f32p]),
     ("nbl_debug_event", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.c_int, C.c_int32, C.c_int64,
