@@ -144,7 +144,9 @@ def cpu_sample(w, cores, per_core):
 def cpu_baseline(w, tri, mats, workdir):
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    sample, n_pix = cpu_sample(w, cores, 20000)
+    # ~10k primaries/s per core: ~15 s of work, so the reference's whole-second
+    # "Simulation" timer is within a few percent
+    sample, n_pix = cpu_sample(w, cores, 150000)
     if os.path.exists(O.REF_CPU_MT):
         rate, sim_s, wall = run_reference_cpu(tri, mats, sample, workdir)
         return {"value": rate, "unit": "primaries/s", "cores": cores, "kind": "reference",
@@ -177,7 +179,7 @@ def reference_arm(args):
     cores = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as d:
         w, tri, mats = make_inputs(d, seed=7)
-        sample, n_pix = cpu_sample(w, cores, 10000)
+        sample, n_pix = cpu_sample(w, cores, 100000)
         for _ in range(args.warmup):
             run_reference_cpu(tri, mats, sample[: max(100, len(sample) // 10)], d)
         rates, secs = [], []
@@ -204,7 +206,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--capacity", type=int, default=1 << 20)
+    ap.add_argument("--capacity", type=int, default=1 << 21)
+    ap.add_argument("--record-capacity", type=int, default=1 << 24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -232,9 +235,11 @@ def main():
         n_pri = len(w.primaries)
         stream = torch.cuda.Stream(device=dev)
         sim = nb.Simulation(g, ms, capacity=args.capacity, seed=1000 + rank, device=dev, tally=w.n_pixels,
-                            stream=stream.cuda_stream)
+                            stream=stream.cuda_stream, record_capacity=args.record_capacity)
         pri_dev = torch.from_numpy(w.primaries.view(np.uint8)).to(f"cuda:{dev}")
         pri_host = torch.from_numpy(w.primaries.view(np.uint8).copy()).pin_memory()
+        rec_host = torch.empty(args.record_capacity * 36, dtype=torch.uint8).pin_memory()
+        rec_view = np.frombuffer(rec_host.numpy(), dtype=nb.PRI_DTYPE)
 
         def step_device():
             sim.reset()
@@ -245,7 +250,7 @@ def main():
             sim.reset()
             sim.push(np.frombuffer(pri_host.numpy(), dtype=nb.PRI_DTYPE))
             sim.run()
-            rec = sim.flush_detected()
+            rec = sim.flush_detected(out=rec_view)
             tal = sim.tallies()
             return rec, tal
 

@@ -262,9 +262,12 @@ class Simulation:
         return n.value
 
     # gpu_driver::flush_buffered: detected electrons as 36-byte records
-    def flush_detected(self):
+    def flush_detected(self, out=None):
+        """Detected records; ``out`` (a PRI_DTYPE array, e.g. over pinned
+        memory) receives them directly when given and large enough."""
         n = self.get_detected_count()
-        out = np.zeros(max(n, 1), PRI_DTYPE)
+        if out is None or len(out) < n:
+            out = np.zeros(max(n, 1), PRI_DTYPE)
         got = C.c_int64()
         check(lib().nbl_sim_drain_detected(self._h, out.ctypes.data, n, C.byref(got)))
         return out[:got.value]

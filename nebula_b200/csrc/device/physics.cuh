@@ -18,6 +18,12 @@
 // Directions are carried unnormalised, as the reference CPU driver stores
 // them, and normalised (sqrt, then multiply by the reciprocal) where used
 // (common/vector_math.h:141-158).
+//
+// Transcendentals use the SFU forms (__logf, __expf, __sincosf; relative
+// errors ~1e-6 for the arguments met here: log of energies and of uniforms,
+// exp of log inverse mean free paths, angles in [-pi, 2 pi]).  The sampled
+// distributions are unchanged at that level; the octree walk and the table
+// lookups, which must match the reference bit for bit, use none of them.
 #pragma once
 #include "../nbl_device_types.h"
 #include "geometry.cuh"
@@ -60,7 +66,7 @@ template<class R> __device__ __forceinline__ float draw_phi(R& rng) { return fm(
 __device__ __forceinline__ V3 make_unit_vec(float cos_theta, float phi)
 {
 	float sp, cp;
-	sincosf(phi, &sp, &cp);
+	__sincosf(phi, &sp, &cp);
 	cos_theta = clampf(cos_theta, -1.0f, 1.0f);
 	const float st = __fsqrt_rn(fs(1.0f, fm(cos_theta, cos_theta)));
 	return v3(fm(st, cp), fm(st, sp), cos_theta);
@@ -75,26 +81,26 @@ template<class R> __device__ __forceinline__ V3 uniform_vector(R& rng)
 __device__ __forceinline__ V3 make_normal_vec(V3 dir, float phi)
 {
 	float sa, ca;
-	sincosf(atan2f(dir.y, dir.x), &sa, &ca);
+	__sincosf(atan2f(dir.y, dir.x), &sa, &ca);
 	const V3 unit_v = v3(fm(dir.z, ca), fm(dir.z, sa), -__fsqrt_rn(fa(fm(dir.x, dir.x), fm(dir.y, dir.y))));
 	const V3 unit_u = vcross(unit_v, dir);
 	float sp, cp;
-	sincosf(phi, &sp, &cp);
+	__sincosf(phi, &sp, &cp);
 	return vadd(vmul(unit_u, cp), vmul(unit_v, sp));
 }
 
 // One exponential free path: -tau * log(U), tau = 1 / (scale * exp(table(log E)))
 template<class R> __device__ __forceinline__ float sample_path(const DevTable& imfp_tab, float scale, float E, R& rng, float& mu)
 {
-	mu = fm(scale, expf(table1_get(imfp_tab, logf(E))));
+	mu = fm(scale, __expf(table1_get(imfp_tab, __logf(E))));
 	const float tau = fd(1.0f, mu);
-	return fm(-tau, logf(rng.unit()));
+	return fm(-tau, __logf(rng.unit()));
 }
 
 // Elastic event (elastic.h:67-115) with acoustic-phonon and atomic-recoil loss.
 template<class R> __device__ __forceinline__ void elastic_event(const DevMaterial& m, Electron& p, R& rng)
 {
-	const float x = logf(p.E);
+	const float x = __logf(p.E);
 	const float y = rng.unit();
 	const float cos_theta = clampf(table2_get(m.el_icdf, x, y), -1.0f, 1.0f);
 	const float sin_theta = __fsqrt_rn(fs(1.0f, fm(cos_theta, cos_theta)));
@@ -115,14 +121,14 @@ template<class R> __device__ __forceinline__ bool inelastic_event(const DevMater
 {
 	float omega;
 	{
-		const float x = logf(p.E);
+		const float x = __logf(p.E);
 		const float y = rng.unit();
-		omega = expf(table2_get(m.in_omega, x, y));
+		omega = __expf(table2_get(m.in_omega, x, y));
 	}
 	float binding;
 	{
-		const float x = logf(p.E);
-		const float y = logf(fd(omega, p.E));
+		const float x = __logf(p.E);
+		const float y = __logf(fd(omega, p.E));
 		const float z = rng.unit();
 		binding = table3_rounddown(m.in_binding, x, y, z);
 	}
@@ -131,7 +137,7 @@ template<class R> __device__ __forceinline__ bool inelastic_event(const DevMater
 		if (omega > m.band_gap) {
 			float q;
 			{
-				const float x = logf(p.E);
+				const float x = __logf(p.E);
 				const float y = fd(omega, p.E);
 				const float z = rng.unit();
 				q = table3_get(m.in_q, x, y, z);

@@ -844,16 +844,32 @@ nbl_status nbl_sim_detected_count(nbl_sim* s, int64_t* n)
 nbl_status nbl_sim_drain_detected(nbl_sim* s, nbl_record* out, int64_t cap, int64_t* n)
 {
 	return guard([&] {
-		require(s && n && (out || cap == 0), "null argument");
+		require(s && n && (out || cap == 0) && cap >= 0, "null argument");
 		set_device(s->device);
-		uint32_t d = 0;
-		CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
-		CU(cudaStreamSynchronize(s->stream));
-		if (d) s->drain_to_host(d);
+		// records parked on the host during the run come first, then the
+		// device buffer is copied straight into the caller's array
 		const int64_t k = std::min<int64_t>(cap, (int64_t)s->host_records.size());
 		if (k > 0) std::memcpy(out, s->host_records.data(), (size_t)k * sizeof(nbl_record));
 		s->host_records.erase(s->host_records.begin(), s->host_records.begin() + k);
-		*n = k;
+		uint32_t d = 0;
+		CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+		d = std::min(d, s->sp.det_cap);
+		int64_t m = 0;
+		if (s->host_records.empty()) {
+			m = std::min<int64_t>(cap - k, (int64_t)d);
+			if (m > 0)
+				CU(cudaMemcpyAsync(out + k, s->detected.p, (size_t)m * sizeof(nbl_record), cudaMemcpyDeviceToHost, s->stream));
+		}
+		if ((int64_t)d > m) {
+			const size_t old = s->host_records.size();
+			s->host_records.resize(old + (d - m));
+			CU(cudaMemcpyAsync(s->host_records.data() + old, s->detected.as<nbl_record>() + m, (size_t)(d - m) * sizeof(nbl_record),
+				cudaMemcpyDeviceToHost, s->stream));
+		}
+		CU(cudaMemsetAsync(s->n_detected.p, 0, sizeof(uint32_t), s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+		*n = k + m;
 	});
 }
 

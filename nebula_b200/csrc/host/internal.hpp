@@ -5,7 +5,7 @@
 #include <map>
 #include <stdexcept>
 #include <cstdint>
-#include "../../../include/nebula_b200.h"
+#include "nebula_b200.h"
 
 namespace nbl {
 

@@ -30,6 +30,13 @@
 #include "device/tables.cuh"
 #include "device/physics.cuh"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
+#ifndef NBL_STEP_MIN_BLOCKS
+#define NBL_STEP_MIN_BLOCKS 4
+#endif
+
 namespace nbl {
 
 __device__ __forceinline__ unsigned lanemask_lt()
@@ -162,9 +169,17 @@ cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, int 
 }
 
 /* ----------------------------------------------------------- transport */
+// Event counters of one block, in shared memory (one shared atomic per
+// counted event), flushed to the device counters once per block and launch.
 struct LocalCounters {
-	uint32_t flights, boundary, elastic, inelastic, spawned, detected, terminated, primaries;
-	uint32_t walk_overflow, nan, queue_overflow, record_overflow, budget, spilled;
+	uint32_t* c;   // shared, N_COUNTERS words
+	// one shared atomic per group of lanes counting together
+	__device__ __forceinline__ void add(int k)
+	{
+		const cg::coalesced_group g = cg::coalesced_threads();
+		if (g.thread_rank() == 0)
+			atomicAdd(c + k, g.size());
+	}
 };
 
 // Free flight(s) from the electron's current state: domain and energy cut,
@@ -178,11 +193,11 @@ __device__ __forceinline__ int free_flight(const StepParams& P, Electron& p, int
 	uint32_t tag, uint64_t lineage, float* sc, LocalCounters& lc)
 {
 	for (int hop = 0; hop < 4; ++hop) {
-		++lc.flights;
-		if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) { ++lc.nan; return -1; }
+		lc.add(CNT_FLIGHTS);
+		if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) { lc.add(CNT_NAN); return -1; }
 		if (!in_domain(P.geom, p.pos.x, p.pos.y, p.pos.z))
 			return -1;
-		if (event >= P.max_events) { ++lc.budget; return -1; }
+		if (event >= P.max_events) { lc.add(CNT_EVENT_BUDGET); return -1; }
 		++event;
 		int type = 0;
 		float dist = P.geom.max_extent;
@@ -203,7 +218,7 @@ __device__ __forceinline__ int free_flight(const StepParams& P, Electron& p, int
 		const V3 d = vnormalised(p.dir);
 		float idist;
 		const int hit = propagate(P.geom, p.pos.x, p.pos.y, p.pos.z, d.x, d.y, d.z, dist, last_tri, mat, idist);
-		if (hit == -2) { ++lc.walk_overflow; return -1; }
+		if (hit == -2) { lc.add(CNT_WALK_OVERFLOW); return -1; }
 		if (ADJ && mat >= 0 && mat < 2) {
 			// score of the flight: density mu_k exp(-(mu_in+mu_el) d) of the
 			// chosen event k at distance d, or survival exp(-(mu_in+mu_el) d)
@@ -235,8 +250,10 @@ __device__ __forceinline__ void store_electron(const Queue& q, uint32_t slot, co
 	q.d[slot] = (uint32_t)(lineage >> 32);
 }
 
+// Four resident blocks of 256 threads per SM (at most 64 registers): the
+// kernel is latency bound, so warps in flight matter more than registers.
 template<bool ADJ>
-__global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
+__global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
 {
 	const uint32_t rs = it % 3u, ws = (it + 1u) % 3u, zs = (it + 2u) % 3u;
 	const uint32_t* cr = P.ctrl + rs * SLOT_WORDS;
@@ -278,7 +295,11 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 	const Queue* qin = P.q[it & 1u];
 	const Queue* qout = P.q[(it + 1u) & 1u];
 
-	LocalCounters lc = {};
+	__shared__ uint32_t s_counters[N_COUNTERS];
+	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
+		s_counters[k] = 0u;
+	__syncthreads();
+	LocalCounters lc{ s_counters };
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -322,7 +343,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 			p.dir = v3(r->dx, r->dy, r->dz);
 			p.E = r->E;
 			tag = qi;
-			++lc.primaries;
+			lc.add(CNT_PRIMARIES);
 		}
 
 		// interaction that ended the previous flight
@@ -330,7 +351,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 		bool spawn = false;
 		Electron se;
 		if (kind == EV_BOUNDARY) {
-			++lc.boundary;
+			lc.add(CNT_BOUNDARY);
 			PhiloxStream r;
 			r.init(P.key, event, 1u, tag, lineage);
 			const DevTriangle T = load_tri(P.geom.tris, last_tri);
@@ -345,13 +366,13 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 				status = boundary_event(T, P.mats, p, mat, r);
 			}
 		} else if (kind == EV_ELASTIC) {
-			++lc.elastic;
+			lc.add(CNT_ELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
 			r.init(P.key, event, 1u, tag, lineage);
 			elastic_event(P.mats[mat], p, r);
 		} else if (kind == EV_INELASTIC) {
-			++lc.inelastic;
+			lc.add(CNT_INELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
 			r.init(P.key, event, 1u, tag, lineage);
@@ -360,7 +381,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 
 		// detection output: record + tallies
 		if (status == ST_DETECTED) {
-			++lc.detected;
+			lc.add(CNT_DETECTED);
 			const Record36* pr = P.primaries + tag;
 			const int px = pr->px, py = pr->py;
 			const Tallies& T = P.tal;
@@ -391,7 +412,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 				rec.px = pr->px; rec.py = pr->py;
 				P.detected[rslot] = rec;
 			} else {
-				++lc.record_overflow;
+				lc.add(CNT_RECORD_OVERFLOW);
 			}
 		}
 
@@ -399,7 +420,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 		// lineage id is derived from the parent's and the spawning event
 		uint64_t se_lineage = 0;
 		if (spawn) {
-			++lc.spawned;
+			lc.add(CNT_SPAWNED);
 			se_lineage = child_lineage(lineage, event);
 		}
 		const uint32_t ticket = warp_reserve(cw + SLOT_TICKETS, spawn);
@@ -412,13 +433,13 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 			uint32_t at = 0;
 			if (queued) {
 				if (sslot < P.qcap) { dst = &qout[EV_NEW]; at = sslot; }
-				else ++lc.queue_overflow;
+				else lc.add(CNT_QUEUE_OVERFLOW);
 			} else {
-				++lc.spilled;
+				lc.add(CNT_SPILLED);
 				// the ring holds at most spill_mask + 1 electrons, counting the
 				// ones being drained during this iteration
 				if (sp_tail + pslot - sp_head <= P.spill_mask) { dst = &P.spill; at = (sp_tail + pslot) & P.spill_mask; }
-				else ++lc.queue_overflow;
+				else lc.add(CNT_QUEUE_OVERFLOW);
 			}
 			if (dst) {
 				store_electron(*dst, at, se, mat, -1, tag, 0u, se_lineage);
@@ -434,7 +455,7 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 		if (status == ST_RUNNING)
 			qtype = free_flight<ADJ>(P, p, mat, last_tri, event, tag, lineage, sc, lc);
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
-			++lc.terminated;
+			lc.add(CNT_TERMINATED);
 #pragma unroll
 		for (int t = 0; t < 3; ++t) {
 			const bool mine = qtype == t;
@@ -447,22 +468,17 @@ __global__ void __launch_bounds__(256) k_step(const StepParams P, uint32_t it)
 						qout[t].s2[slot] = make_float2(sc[4], sc[5]);
 					}
 				} else {
-					++lc.queue_overflow;
+					lc.add(CNT_QUEUE_OVERFLOW);
 				}
 			}
 		}
 	}
 
-	// flush counters: one atomic per warp and counter
-	const uint32_t vals[N_COUNTERS] = { lc.flights, lc.boundary, lc.elastic, lc.inelastic, lc.spawned,
-		lc.detected, lc.terminated, lc.primaries, lc.walk_overflow, lc.nan, lc.queue_overflow,
-		lc.record_overflow, lc.budget, lc.spilled };
-#pragma unroll
-	for (int k = 0; k < N_COUNTERS; ++k) {
-		const uint32_t v = __reduce_add_sync(0xffffffffu, vals[k]);
-		if (lane == 0 && v)
-			atomicAdd(P.counters + k, (unsigned long long)v);
-	}
+	// flush the block's counters: one global atomic per block and counter
+	__syncthreads();
+	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
+		if (s_counters[k])
+			atomicAdd(P.counters + k, (unsigned long long)s_counters[k]);
 }
 
 cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)
