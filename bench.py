@@ -199,6 +199,76 @@ def reference_arm(args):
         "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+# ---------------------------------------------------------------------------- batch
+def batched_vs_plain(args, dev, workdir):
+    """The mixed 64-job batch: one persistent batched launch against the
+    plain wavefront run job by job (one pool reused per geometry; pool
+    creation not timed), same seeds, so per-job yields must be identical.
+    Batch parameters come from the autotuner's stored choice when present."""
+    import torch
+    import nebula_b200 as nb
+    from nebula_b200 import autotune
+    from nebula_b200.tune_mixed_batch import load_mixed_batch, OUT as TUNED
+    geoms, mats, jobs, desc = load_mixed_batch(workdir)
+    n_pri = sum(len(p) for _, _, p in jobs)
+    if os.path.exists(TUNED):
+        best = autotune.load(TUNED)
+        params = dict(capacity=int(best["capacity"]), block=int(best["block"]), threshold=float(best["threshold"]),
+                      source="autotuner (nebula_b200/tuned/mixed_batch.json)")
+    else:
+        params = dict(capacity=1 << 22, block=512, threshold=0.5, source="default")
+    b = nb.Batch(geoms, mats, capacity=params["capacity"], block_size=params["block"],
+                 refill_threshold=params["threshold"], device=dev)
+    b.set_jobs(jobs)
+    b.run()                                     # warm-up
+    batch_ms = []
+    for _ in range(args.steps):
+        b.run()
+        batch_ms.append(b.kernel_ms())
+    c = b.counters()
+    se_b, bse_b = b.job_yields()
+    b.close()
+
+    def plain_pass():
+        se, ms_dev, wall = [], 0.0, 0.0
+        cur = None
+        for gi, seed, pri in jobs:
+            if cur is None or cur[0] != gi:
+                if cur is not None:
+                    cur[1].close()
+                cur = (gi, nb.Simulation(geoms[gi], mats[: (1 if gi == 0 else 2)], capacity=1 << 20, seed=seed,
+                                         record_capacity=1 << 24, device=dev))
+            s = cur[1]
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            s.reset()
+            s.set_seed(seed)
+            s.push(pri)
+            s.run()
+            rec = s.flush_detected()
+            wall += time.perf_counter() - t0
+            ms_dev += s.kernel_ms()
+            se.append(int((rec["E"] < 50).sum()))
+        cur[1].close()
+        return np.array(se), wall, ms_dev
+
+    plain_pass()                                # warm-up
+    walls, devs = [], []
+    for _ in range(args.steps):
+        se_p, w, m = plain_pass()
+        walls.append(w)
+        devs.append(m)
+    bm = float(np.mean(batch_ms)) / 1e3
+    pw = float(np.mean(walls))
+    return {"workload": "mixed batch: %d jobs, %d primaries (slab / gratings pitch 20-64 nm, 200 eV-20 keV, "
+                        "1e3-1e6 primaries per job)" % (len(jobs), n_pri),
+            "value": n_pri / bm, "unit": "primaries/s", "seconds": bm,
+            "plain_value": n_pri / pw, "plain_seconds": pw, "plain_transport_seconds": float(np.mean(devs)) / 1e3,
+            "ratio_batched_over_plain": pw / bm, "flights": c["flights"], "iterations": c["iterations"],
+            "spilled": c["spilled"], "per_job_yields_identical": bool(np.array_equal(se_b, se_p)),
+            "params": params, "launches_per_run": 1}
+
+
 # ---------------------------------------------------------------------------- GPU
 def main():
     ap = argparse.ArgumentParser()
@@ -209,6 +279,7 @@ def main():
     ap.add_argument("--capacity", type=int, default=1 << 21)
     ap.add_argument("--record-capacity", type=int, default=1 << 24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch (batched vs plain) measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -302,7 +373,6 @@ def main():
             t = torch.tensor([e2e_ms], device=f"cuda:{dev}")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_ms = float(t.item())
-        sim.close()
 
         value = n_pri * args.steps * world / (ms / 1000.0)
         e2e_value = n_pri * args.steps * world / (e2e_ms / 1000.0)
@@ -326,6 +396,9 @@ def main():
             "gpu_launches": iters,
             "clocks": clk.summary(),
         }
+        sim.close()
+        if not args.no_batch:
+            out["batched"] = batched_vs_plain(args, dev, d)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             try:
                 out["cpu_baseline"] = cpu_baseline(w, tri, mats, d)

@@ -229,10 +229,60 @@ nbl_status nbl_sim_counters(nbl_sim* s, nbl_counters* out);
 /* Clear tallies, counters and records, forget pushed primaries, keep geometry
  * and materials (a new scan on the same sample). */
 nbl_status nbl_sim_reset(nbl_sim* s);
+/* Change the random-number key for the next run (e.g. a new scan on the same
+ * sample); call between runs. */
+nbl_status nbl_sim_set_seed(nbl_sim* s, uint64_t seed);
 /* Device time of the transport iterations run so far (CUDA events around
  * each graph launch), milliseconds. */
 nbl_status nbl_sim_kernel_ms(nbl_sim* s, double* ms);
 void nbl_sim_destroy(nbl_sim* s);
+
+/* ------------------------------------------------------------ batched runs */
+/* Many scan jobs -- each with its own geometry, primaries and seed -- fed
+ * into one electron pool by a persistent kernel: every wavefront iteration of
+ * the whole batch runs inside ONE cooperative launch (a grid barrier between
+ * iterations instead of a kernel boundary), captured in a CUDA graph.  The
+ * reference runs one scan at a time through gpu_driver (gpu_main.cu:92-232);
+ * a job's electrons here draw exactly the random numbers a plain run of that
+ * job alone with the same seed draws, so per-job results equal the plain
+ * run's. */
+typedef struct nbl_batch_job {
+	int32_t geometry;          /* index into the geometries given to nbl_batch_create */
+	uint32_t reserved;
+	uint64_t seed;             /* the job's random-number key (as nbl_params.seed) */
+	int64_t first;             /* first primary of the job in the batch's primary array */
+	int64_t count;             /* its number of primaries (< 2^24) */
+} nbl_batch_job;
+
+typedef struct nbl_batch_params {
+	int32_t device;
+	uint32_t capacity;         /* refill target (electrons); 0: 1 << 20 */
+	float refill_threshold;    /* refill only while fewer than threshold x capacity are in flight; 0: 1 */
+	uint32_t block_size;       /* 128, 256 or 512; 0: 256 */
+	uint32_t queue_factor;     /* population bound = factor x capacity; 0: 4 */
+	float energy_threshold;
+	uint32_t max_events;       /* per-electron flight budget; 0: 1 << 22 */
+	uint32_t max_iterations;   /* iteration bound of one launch; 0: 1 << 20 */
+	int32_t use_graph;         /* capture the launch in a CUDA graph; 0: plain launch */
+	void* stream;              /* NULL: a library-owned stream */
+} nbl_batch_params;
+void nbl_batch_params_defaults(nbl_batch_params* p);
+
+typedef struct nbl_batch nbl_batch;
+nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geometries,
+	nbl_material* const* materials, int32_t n_materials, const nbl_batch_params* params, nbl_batch** out);
+/* Jobs and the batch's primary array (host records, copied; each job's range
+ * [first, first+count) must lie inside it, ranges in increasing order). */
+nbl_status nbl_batch_set_jobs(nbl_batch* b, const nbl_batch_job* jobs, int32_t n_jobs, const nbl_record* primaries,
+	int64_t n_primaries);
+/* Run every job to completion in one persistent launch. */
+nbl_status nbl_batch_run(nbl_batch* b);
+/* Detected electrons per job: se (E < 50 eV) and bse (E >= 50 eV), n_jobs each. */
+nbl_status nbl_batch_job_yields(nbl_batch* b, uint64_t* se, uint64_t* bse);
+nbl_status nbl_batch_counters(nbl_batch* b, nbl_counters* out);
+/* Device time of the last run (CUDA events around the launch), ms. */
+nbl_status nbl_batch_kernel_ms(nbl_batch* b, double* ms);
+void nbl_batch_destroy(nbl_batch* b);
 
 /* ------------------------------------------------------------ run without allocation */
 /* No counterpart in the reference.  For callers that cannot allocate device

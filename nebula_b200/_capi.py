@@ -68,6 +68,18 @@ class Params(C.Structure):
                 ("physics", PhysicsOpts), ("adjoint", C.c_int32)]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("geometry", C.c_int32), ("reserved", C.c_uint32), ("seed", C.c_uint64), ("first", C.c_int64),
+                ("count", C.c_int64)]
+
+
+class BatchParams(C.Structure):
+    _fields_ = [("device", C.c_int32), ("capacity", C.c_uint32), ("refill_threshold", C.c_float),
+                ("block_size", C.c_uint32), ("queue_factor", C.c_uint32), ("energy_threshold", C.c_float),
+                ("max_events", C.c_uint32), ("max_iterations", C.c_uint32), ("use_graph", C.c_int32),
+                ("stream", C.c_void_p)]
+
+
 COUNTER_NAMES = ("flights", "boundary", "elastic", "inelastic", "spawned", "detected", "terminated",
                  "primaries_started", "walk_overflow", "nan_state", "queue_overflow",
                  "record_overflow", "event_budget", "spilled", "iterations", "primaries_total",
@@ -110,8 +122,18 @@ _DECLS = [
     ("nbl_sim_tallies", C.c_int, [C.c_void_p, u32p, u32p, u32p]),
     ("nbl_sim_counters", C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     ("nbl_sim_reset", C.c_int, [C.c_void_p]),
+    ("nbl_sim_set_seed", C.c_int, [C.c_void_p, C.c_uint64]),
     ("nbl_sim_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_destroy", None, [C.c_void_p]),
+    ("nbl_batch_params_defaults", None, [C.POINTER(BatchParams)]),
+    ("nbl_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.c_int32,
+                                   C.POINTER(BatchParams), C.POINTER(C.c_void_p)]),
+    ("nbl_batch_set_jobs", C.c_int, [C.c_void_p, C.POINTER(BatchJob), C.c_int32, C.c_void_p, C.c_int64]),
+    ("nbl_batch_run", C.c_int, [C.c_void_p]),
+    ("nbl_batch_job_yields", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("nbl_batch_counters", C.c_int, [C.c_void_p, C.POINTER(Counters)]),
+    ("nbl_batch_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("nbl_batch_destroy", None, [C.c_void_p]),
     ("nbl_run_noalloc", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(Params), C.c_void_p,
                                   C.c_int64, C.c_void_p, C.c_int64, i64p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(Counters)]),

@@ -293,12 +293,92 @@ class Simulation:
         check(lib().nbl_sim_kernel_ms(self._h, C.byref(v)))
         return v.value
 
+    def set_seed(self, seed):
+        check(lib().nbl_sim_set_seed(self._h, seed))
+
     def reset(self):
         check(lib().nbl_sim_reset(self._h))
 
     def close(self):
         if getattr(self, "_h", None):
             lib().nbl_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many scan jobs (own geometry, primaries and seed each) in one
+    persistent launch.  A job's electrons draw the random numbers a plain
+    ``Simulation`` of that job alone with the job's seed draws, so per-job
+    results equal the plain run's."""
+
+    def __init__(self, geometries, materials, capacity=1 << 20, refill_threshold=1.0, block_size=256,
+                 queue_factor=4, device=0, use_graph=True, energy_threshold=0.0, max_events=0, stream=None):
+        p = _capi.BatchParams()
+        lib().nbl_batch_params_defaults(C.byref(p))
+        p.device = device
+        p.capacity = capacity
+        p.refill_threshold = refill_threshold
+        p.block_size = block_size
+        p.queue_factor = queue_factor
+        p.use_graph = int(bool(use_graph))
+        p.energy_threshold = energy_threshold
+        p.max_events = max_events
+        p.stream = stream
+        self.params = p
+        self.geometries = list(geometries)
+        self.materials = list(materials)
+        ga = (C.c_void_p * len(self.geometries))(*[g._h.value if isinstance(g._h, C.c_void_p) else g._h
+                                                   for g in self.geometries])
+        ma = (C.c_void_p * len(self.materials))(*[m._h.value if isinstance(m._h, C.c_void_p) else m._h
+                                                  for m in self.materials])
+        h = C.c_void_p()
+        check(lib().nbl_batch_create(ga, len(self.geometries), ma, len(self.materials), C.byref(p), C.byref(h)))
+        self._h = h
+        self.n_jobs = 0
+
+    def set_jobs(self, jobs):
+        """``jobs``: list of (geometry index, seed, PRI_DTYPE primaries)."""
+        arr = (_capi.BatchJob * len(jobs))()
+        first = 0
+        for i, (gi, seed, pri) in enumerate(jobs):
+            arr[i].geometry = gi
+            arr[i].seed = seed
+            arr[i].first = first
+            arr[i].count = len(pri)
+            first += len(pri)
+        allp = np.ascontiguousarray(np.concatenate([np.asarray(p, PRI_DTYPE) for _, _, p in jobs]), PRI_DTYPE)
+        check(lib().nbl_batch_set_jobs(self._h, arr, len(jobs), allp.ctypes.data, len(allp)))
+        self.n_jobs = len(jobs)
+        self.n_primaries = len(allp)
+
+    def run(self):
+        check(lib().nbl_batch_run(self._h))
+
+    def job_yields(self):
+        se = (C.c_uint64 * self.n_jobs)()
+        bse = (C.c_uint64 * self.n_jobs)()
+        check(lib().nbl_batch_job_yields(self._h, se, bse))
+        return np.array(se[:], np.int64), np.array(bse[:], np.int64)
+
+    def counters(self):
+        c = _capi.Counters()
+        check(lib().nbl_batch_counters(self._h, C.byref(c)))
+        return {n: int(getattr(c, n)) for n in _capi.COUNTER_NAMES}
+
+    def kernel_ms(self):
+        v = C.c_double()
+        check(lib().nbl_batch_kernel_ms(self._h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nbl_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -69,6 +69,31 @@ struct StepParams {
 	unsigned long long* counters;
 	uint32_t max_events;      // per-electron event budget
 	int32_t adjoint;          // accumulate score functions
+	uint32_t refill_below;    // refill primaries only while fewer electrons are in flight
+};
+
+// One job of a batched run: its geometry, its primaries (a contiguous range
+// of the batch's primary array) and its random-number key.
+struct DevJob {
+	uint32_t geom;
+	uint32_t first;
+	uint32_t count;
+	PhiloxKey key;
+	uint32_t pad;
+};
+
+// Per-job state of a batched (persistent) run.
+struct BatchParams {
+	const DevGeometry* geoms;
+	const DevJob* jobs;
+	int32_t n_jobs;
+	unsigned long long* job_se;     // detected with E < 50 eV, per job
+	unsigned long long* job_bse;    // detected with E >= 50 eV, per job
+	uint32_t* bar_count;            // grid barrier arrival counter
+	uint32_t* bar_gen;              // grid barrier generation
+	uint32_t* err;                  // bit 0: barrier timeout, bit 1: iteration bound
+	uint32_t* iterations;           // iterations the launch ran
+	uint32_t max_iterations;
 };
 
 // launchers
@@ -83,5 +108,7 @@ cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, int 
 	cudaStream_t s);
 cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s);
 int step_grid_size(int device, int block);
+cudaError_t launch_batch(const StepParams& p, const BatchParams& b, int grid, int block, cudaStream_t s);
+int batch_grid_size(int device, int block);
 
 }  // namespace nbl

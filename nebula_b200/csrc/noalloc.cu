@@ -225,6 +225,7 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		sp.qcap = 8 * cap;
 		sp.capacity = cap;
 		sp.ramp = std::max<uint32_t>(cap / 16, 256);
+		sp.refill_below = cap;
 		sp.spill = carve_queue(base + OFF_SPILL, NA_RING);
 		sp.spill_mask = NA_RING - 1;
 		sp.ctrl = reinterpret_cast<uint32_t*>(base + OFF_CTRL);

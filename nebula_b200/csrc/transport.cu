@@ -182,6 +182,13 @@ struct LocalCounters {
 	}
 };
 
+// What one electron needs to know about the run it belongs to: its geometry
+// and its random-number key (a batched run holds one of each per job).
+struct RunView {
+	const DevGeometry* geom;
+	PhiloxKey key;
+};
+
 // Free flight(s) from the electron's current state: domain and energy cut,
 // free-path sampling, octree walk, move.  Flights in vacuum that hit nothing
 // end without an event and are repeated (the next one leaves the domain).
@@ -189,18 +196,19 @@ struct LocalCounters {
 // is terminated.  Mirrors cpu_driver::init / kernels::init
 // (drivers/cpu/cpu_driver.inl:74-130, drivers/gpu/gpu_driver.inl:403-480).
 template<bool ADJ>
-__device__ __forceinline__ int free_flight(const StepParams& P, Electron& p, int mat, int& last_tri, uint32_t& event,
-	uint32_t tag, uint64_t lineage, float* sc, LocalCounters& lc)
+__device__ __forceinline__ int free_flight(const StepParams& P, const RunView& rv, Electron& p, int mat, int& last_tri,
+	uint32_t& event, uint32_t stream_tag, uint64_t lineage, float* sc, LocalCounters& lc)
 {
+	const DevGeometry& G = *rv.geom;
 	for (int hop = 0; hop < 4; ++hop) {
 		lc.add(CNT_FLIGHTS);
 		if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) { lc.add(CNT_NAN); return -1; }
-		if (!in_domain(P.geom, p.pos.x, p.pos.y, p.pos.z))
+		if (!in_domain(G, p.pos.x, p.pos.y, p.pos.z))
 			return -1;
 		if (event >= P.max_events) { lc.add(CNT_EVENT_BUDGET); return -1; }
 		++event;
 		int type = 0;
-		float dist = P.geom.max_extent;
+		float dist = G.max_extent;
 		float mu_el = 0.0f, mu_in = 0.0f;
 		const DevMaterial* m = nullptr;
 		if (mat >= 0) {
@@ -208,7 +216,7 @@ __device__ __forceinline__ int free_flight(const StepParams& P, Electron& p, int
 			if (p.E < fa(m->barrier, P.energy_threshold))
 				return -1;
 			PhiloxStream r;
-			r.init(P.key, event, 0u, tag, lineage);
+			r.init(rv.key, event, 0u, stream_tag, lineage);
 			const float pe = sample_path(m->el_imfp, m->el_scale, p.E, r, mu_el);
 			const float pi = sample_path(m->in_imfp, m->in_scale, p.E, r, mu_in);
 			dist = __int_as_float(0x7f800000);
@@ -217,7 +225,7 @@ __device__ __forceinline__ int free_flight(const StepParams& P, Electron& p, int
 		}
 		const V3 d = vnormalised(p.dir);
 		float idist;
-		const int hit = propagate(P.geom, p.pos.x, p.pos.y, p.pos.z, d.x, d.y, d.z, dist, last_tri, mat, idist);
+		const int hit = propagate(G, p.pos.x, p.pos.y, p.pos.z, d.x, d.y, d.z, dist, last_tri, mat, idist);
 		if (hit == -2) { lc.add(CNT_WALK_OVERFLOW); return -1; }
 		if (ADJ && mat >= 0 && mat < 2) {
 			// score of the flight: density mu_k exp(-(mu_in+mu_el) d) of the
@@ -250,29 +258,52 @@ __device__ __forceinline__ void store_electron(const Queue& q, uint32_t slot, co
 	q.d[slot] = (uint32_t)(lineage >> 32);
 }
 
-// Four resident blocks of 256 threads per SM (at most 64 registers): the
-// kernel is latency bound, so warps in flight matter more than registers.
-template<bool ADJ>
-__global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
+// Loads of data written during the same launch by other SMs bypass L1
+// (the persistent kernel keeps running across iterations).
+__device__ __forceinline__ uint32_t ld_ctrl(const uint32_t* p) { return __ldcg(p); }
+
+// Job of a batched primary (global index g): the last job whose first
+// primary is <= g.
+__device__ __forceinline__ uint32_t job_of(const BatchParams& B, uint32_t g)
+{
+	int lo = 0, hi = B.n_jobs - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (__ldg(&B.jobs[mid].first) <= g) lo = mid; else hi = mid - 1;
+	}
+	return (uint32_t)lo;
+}
+
+// One wavefront iteration over the index space
+//   [boundary | elastic | inelastic | new secondaries | drained ring | primaries].
+// Returns false when there was no work at all (the run is finished); every
+// thread of every block sees the same control words and returns the same.
+// BATCH: electrons carry their job in the tag's top 8 bits (the low 24 bits
+// are the primary's index within its job, which keys its random numbers, as
+// in a run of that job alone); geometry, key and yield tallies are per job.
+template<bool ADJ, bool BATCH>
+__device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc)
 {
 	const uint32_t rs = it % 3u, ws = (it + 1u) % 3u, zs = (it + 2u) % 3u;
 	const uint32_t* cr = P.ctrl + rs * SLOT_WORDS;
 	uint32_t* cw = P.ctrl + ws * SLOT_WORDS;
 	// counts are clamped to the queue capacity (the secondary budget below
 	// keeps them there; the clamp makes an out-of-range read impossible)
-	const uint32_t n0 = min(cr[0], P.qcap), n1 = min(cr[1], P.qcap), n2 = min(cr[2], P.qcap), n3 = min(cr[3], P.qcap);
-	const uint32_t cursor = cr[SLOT_CURSOR];
+	const uint32_t n0 = min(ld_ctrl(cr + 0), P.qcap), n1 = min(ld_ctrl(cr + 1), P.qcap);
+	const uint32_t n2 = min(ld_ctrl(cr + 2), P.qcap), n3 = min(ld_ctrl(cr + 3), P.qcap);
+	const uint32_t cursor = ld_ctrl(cr + SLOT_CURSOR);
 	const uint32_t e1 = n0 + n1, e2 = e1 + n2, active = e2 + n3;
 	// spill ring: secondaries that found no room earlier, drained (oldest
 	// first) ahead of new primaries while the population has room
-	const uint32_t sp_head = cr[SLOT_SPILL_HEAD];
-	const uint32_t sp_tail = cr[SLOT_SPILL_TAIL] + cr[SLOT_SPILL_PUSHED];
+	const uint32_t sp_head = ld_ctrl(cr + SLOT_SPILL_HEAD);
+	const uint32_t sp_tail = ld_ctrl(cr + SLOT_SPILL_TAIL) + ld_ctrl(cr + SLOT_SPILL_PUSHED);
 	const uint32_t sp_room = active < P.qcap ? P.qcap - active : 0u;
 	const uint32_t n_drain = min(sp_tail - sp_head, sp_room);
 	const uint32_t e3 = active + n_drain;
-	// no new primaries while secondaries are still parked in the ring
+	// no new primaries while secondaries are still parked in the ring, nor
+	// while the population is above the refill threshold
 	const bool parked = sp_tail - sp_head > n_drain;
-	const uint32_t room = (e3 < P.capacity && !parked) ? P.capacity - e3 : 0u;
+	const uint32_t room = (e3 < P.refill_below && !parked) ? P.capacity - min(e3, P.capacity) : 0u;
 	const uint32_t left = P.n_primaries - cursor;
 	const uint32_t nr = min(min(room, left), P.ramp);
 	const uint32_t total = e3 + nr;
@@ -292,14 +323,13 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 		for (int k = 0; k < SLOT_WORDS; ++k)
 			cz[k] = 0u;
 	}
+	// an iteration without work still carries cursor and ring state forward
+	// (above), so iterations launched after the end stay empty
+	if (total == 0u)
+		return false;
 	const Queue* qin = P.q[it & 1u];
 	const Queue* qout = P.q[(it + 1u) & 1u];
 
-	__shared__ uint32_t s_counters[N_COUNTERS];
-	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
-		s_counters[k] = 0u;
-	__syncthreads();
-	LocalCounters lc{ s_counters };
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -326,15 +356,15 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 		for (int k = 0; k < 6; ++k) sc[k] = 0.0f;
 		if (kind == 5 || (kind >= 0 && kind < 4)) {
 			const Queue& q = kind == 5 ? P.spill : qin[kind];
-			const float4 a = q.a[qi], b = q.b[qi];
-			const uint4 c = q.c[qi];
+			const float4 a = __ldcg(q.a + qi), b = __ldcg(q.b + qi);
+			const uint4 c = __ldcg(q.c + qi);
 			p.pos = v3(a.x, a.y, a.z); p.E = a.w;
 			p.dir = v3(b.x, b.y, b.z); mat = __float_as_int(b.w);
 			last_tri = (int)c.x; tag = c.y; event = c.z;
-			lineage = ((uint64_t)q.d[qi] << 32) | c.w;
+			lineage = ((uint64_t)__ldcg(q.d + qi) << 32) | c.w;
 			if (ADJ) {
-				const float4 s = q.s[qi];
-				const float2 s2 = q.s2[qi];
+				const float4 s = __ldcg(q.s + qi);
+				const float2 s2 = __ldcg(q.s2 + qi);
 				sc[0] = s.x; sc[1] = s.y; sc[2] = s.z; sc[3] = s.w; sc[4] = s2.x; sc[5] = s2.y;
 			}
 		} else if (kind == 4) {
@@ -342,8 +372,29 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 			p.pos = v3(r->x, r->y, r->z);
 			p.dir = v3(r->dx, r->dy, r->dz);
 			p.E = r->E;
-			tag = qi;
+			if (BATCH) {
+				const uint32_t j = job_of(B, qi);
+				tag = (j << 24) | (qi - __ldg(&B.jobs[j].first));
+			} else {
+				tag = qi;
+			}
 			lc.add(CNT_PRIMARIES);
+		}
+		// run context: job geometry / key, the primary's record, the tag that
+		// keys the random numbers
+		RunView rv;
+		uint32_t job = 0, stream_tag = tag, rec_index = tag;
+		if (BATCH) {
+			job = tag >> 24;
+			stream_tag = tag & 0xFFFFFFu;
+			const DevJob* J = B.jobs + (kind >= 0 ? job : 0u);
+			rv.geom = B.geoms + __ldg(&J->geom);
+			rv.key.k0 = __ldg(&J->key.k0);
+			rv.key.k1 = __ldg(&J->key.k1);
+			rec_index = __ldg(&J->first) + stream_tag;
+		} else {
+			rv.geom = &P.geom;
+			rv.key = P.key;
 		}
 
 		// interaction that ended the previous flight
@@ -353,8 +404,8 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 		if (kind == EV_BOUNDARY) {
 			lc.add(CNT_BOUNDARY);
 			PhiloxStream r;
-			r.init(P.key, event, 1u, tag, lineage);
-			const DevTriangle T = load_tri(P.geom.tris, last_tri);
+			r.init(rv.key, event, 1u, stream_tag, lineage);
+			const DevTriangle T = load_tri(rv.geom->tris, last_tri);
 			if (ADJ) {
 				BoundaryScore bs = { 0.0f, 0.0f, -1, -1 };
 				status = boundary_event(T, P.mats, p, mat, r, &bs);
@@ -369,30 +420,34 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 			lc.add(CNT_ELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
-			r.init(P.key, event, 1u, tag, lineage);
+			r.init(rv.key, event, 1u, stream_tag, lineage);
 			elastic_event(P.mats[mat], p, r);
 		} else if (kind == EV_INELASTIC) {
 			lc.add(CNT_INELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
-			r.init(P.key, event, 1u, tag, lineage);
+			r.init(rv.key, event, 1u, stream_tag, lineage);
 			spawn = inelastic_event(P.mats[mat], p, se, r);
 		}
 
 		// detection output: record + tallies
 		if (status == ST_DETECTED) {
 			lc.add(CNT_DETECTED);
-			const Record36* pr = P.primaries + tag;
-			const int px = pr->px, py = pr->py;
 			const Tallies& T = P.tal;
-			if (T.se_img && px >= 0 && py >= 0 && px < T.nx && py < T.ny) {
-				const size_t pix = (size_t)py * T.nx + px;
-				atomicAdd((p.E < 50.0f ? T.se_img : T.bse_img) + pix, 1u);
-				if (ADJ && T.grad_se) {
-					double* g = (p.E < 50.0f ? T.grad_se : T.grad_bse) + pix * 6;
+			if (BATCH) {
+				atomicAdd((p.E < 50.0f ? B.job_se : B.job_bse) + job, 1ull);
+			} else {
+				const Record36* pr = P.primaries + rec_index;
+				const int px = pr->px, py = pr->py;
+				if (T.se_img && px >= 0 && py >= 0 && px < T.nx && py < T.ny) {
+					const size_t pix = (size_t)py * T.nx + px;
+					atomicAdd((p.E < 50.0f ? T.se_img : T.bse_img) + pix, 1u);
+					if (ADJ && T.grad_se) {
+						double* g = (p.E < 50.0f ? T.grad_se : T.grad_bse) + pix * 6;
 #pragma unroll
-					for (int k = 0; k < 6; ++k)
-						atomicAdd(g + k, (double)sc[k]);
+						for (int k = 0; k < 6; ++k)
+							atomicAdd(g + k, (double)sc[k]);
+					}
 				}
 			}
 			if (T.hist && p.E >= 0.0f && p.E < T.hist_emax) {
@@ -401,18 +456,20 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 				atomicAdd(T.hist + bin, 1u);
 			}
 		}
-		const bool det = status == ST_DETECTED;
-		const uint32_t rslot = warp_reserve(P.n_detected, det);
-		if (det) {
-			if (rslot < P.det_cap) {
-				Record36 rec;
-				const Record36* pr = P.primaries + tag;
-				rec.x = p.pos.x; rec.y = p.pos.y; rec.z = p.pos.z;
-				rec.dx = p.dir.x; rec.dy = p.dir.y; rec.dz = p.dir.z; rec.E = p.E;
-				rec.px = pr->px; rec.py = pr->py;
-				P.detected[rslot] = rec;
-			} else {
-				lc.add(CNT_RECORD_OVERFLOW);
+		if (P.detected) {
+			const bool det = status == ST_DETECTED;
+			const uint32_t rslot = warp_reserve(P.n_detected, det);
+			if (det) {
+				if (rslot < P.det_cap) {
+					Record36 rec;
+					const Record36* pr = P.primaries + rec_index;
+					rec.x = p.pos.x; rec.y = p.pos.y; rec.z = p.pos.z;
+					rec.dx = p.dir.x; rec.dy = p.dir.y; rec.dz = p.dir.z; rec.E = p.E;
+					rec.px = pr->px; rec.py = pr->py;
+					P.detected[rslot] = rec;
+				} else {
+					lc.add(CNT_RECORD_OVERFLOW);
+				}
 			}
 		}
 
@@ -453,7 +510,7 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 		// next free flight
 		int qtype = -1;
 		if (status == ST_RUNNING)
-			qtype = free_flight<ADJ>(P, p, mat, last_tri, event, tag, lineage, sc, lc);
+			qtype = free_flight<ADJ>(P, rv, p, mat, last_tri, event, stream_tag, lineage, sc, lc);
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
 			lc.add(CNT_TERMINATED);
 #pragma unroll
@@ -473,12 +530,91 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 			}
 		}
 	}
+	return true;
+}
 
-	// flush the block's counters: one global atomic per block and counter
+__device__ __forceinline__ void flush_counters(const StepParams& P, uint32_t* s_counters)
+{
 	__syncthreads();
 	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
 		if (s_counters[k])
 			atomicAdd(P.counters + k, (unsigned long long)s_counters[k]);
+}
+
+// One wavefront iteration per launch (the plain method).  Four resident
+// blocks of 256 threads per SM (at most 64 registers): the kernel is latency
+// bound, so warps in flight matter more than registers.
+template<bool ADJ>
+__global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
+{
+	__shared__ uint32_t s_counters[N_COUNTERS];
+	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
+		s_counters[k] = 0u;
+	__syncthreads();
+	LocalCounters lc{ s_counters };
+	const BatchParams none{};
+	step_iteration<ADJ, false>(P, none, it, lc);
+	flush_counters(P, s_counters);
+}
+
+// Grid-wide barrier of the persistent kernel (all blocks co-resident by the
+// cooperative launch).  Arrival counter + generation word; waiting is bounded
+// (2^22 polls, a few seconds; one iteration takes milliseconds); on timeout,
+// or if any block already timed out, it records the error and returns false
+// so every block leaves.
+__device__ __forceinline__ bool grid_barrier(const BatchParams& B)
+{
+	__shared__ int s_ok;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		const unsigned gen0 = atomicAdd(B.bar_gen, 0u);
+		__threadfence();
+		const unsigned arrived = atomicAdd(B.bar_count, 1u) + 1u;
+		int ok = 1;
+		if (arrived == gridDim.x) {
+			atomicExch(B.bar_count, 0u);
+			__threadfence();
+			atomicAdd(B.bar_gen, 1u);
+		} else {
+			unsigned polls = 0;
+			while (atomicAdd(B.bar_gen, 0u) == gen0) {
+				if (atomicAdd(B.err, 0u)) { ok = 0; break; }
+				__nanosleep(64);
+				if (++polls > (1u << 22)) { atomicOr(B.err, 1u); ok = 0; break; }
+			}
+		}
+		__threadfence();
+		s_ok = ok && atomicAdd(B.err, 0u) == 0u;
+	}
+	__syncthreads();
+	return s_ok != 0;
+}
+
+// The batched method: one persistent launch runs every iteration of a whole
+// batch of jobs, with a grid barrier between iterations instead of a kernel
+// boundary; it ends when an iteration finds no work (all blocks see the same
+// control words) or after max_iterations (error word set).
+template<bool ADJ>
+__global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const BatchParams B)
+{
+	__shared__ uint32_t s_counters[N_COUNTERS];
+	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
+		s_counters[k] = 0u;
+	__syncthreads();
+	LocalCounters lc{ s_counters };
+	uint32_t it = 0;
+	for (; it < B.max_iterations; ++it) {
+		if (!step_iteration<ADJ, true>(P, B, it, lc))
+			break;
+		if (!grid_barrier(B))
+			break;
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		*B.iterations = it;
+		if (it >= B.max_iterations)
+			atomicOr(B.err, 2u);
+	}
+	flush_counters(P, s_counters);
 }
 
 cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)
@@ -498,6 +634,21 @@ int step_grid_size(int device, int block)
 	if (per_sm < 1)
 		per_sm = 1;
 	return sms * per_sm;
+}
+
+int batch_grid_size(int device, int block)
+{
+	int sms = 148, per_sm = 0;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<false>, block, 0);
+	return sms * per_sm;
+}
+
+cudaError_t launch_batch(const StepParams& p, const BatchParams& b, int grid, int block, cudaStream_t s)
+{
+	void* args[] = { const_cast<StepParams*>(&p), const_cast<BatchParams*>(&b) };
+	return cudaLaunchCooperativeKernel((const void*)(p.adjoint ? k_batch<true> : k_batch<false>), dim3(grid), dim3(block),
+		args, 0, s);
 }
 
 }  // namespace nbl

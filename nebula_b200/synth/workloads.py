@@ -79,3 +79,38 @@ def batch_jobs(n_jobs=64, seed=2024, e_lo=200.0, e_hi=20e3, n_lo=1e3, n_hi=1e6):
 
 def adjoint(nx=64, ny=64, per_pixel=10_000, energy=500.0):
     return grating(nx=nx, ny=ny, per_pixel=per_pixel, energy=energy)
+
+
+def batch(seed=2024, n_jobs=64, scale=1.0, e_max=30e3):
+    """The mixed batch: geometries (slab first, then one grating per distinct
+    pitch), material specs covering the energy range, and jobs as
+    (geometry index, seed, primaries).  ``scale`` multiplies every job's
+    primary count (a bounded sample of the batch keeps its energy and
+    geometry mix).  Slab jobs: a point beam at (0, 0, +5 nm); grating jobs:
+    primaries spread uniformly over a 64 x 64 nm field centred on the lines,
+    starting at z = 40 nm; all at normal incidence."""
+    desc = batch_jobs(n_jobs=n_jobs, seed=seed)
+    geoms = [geometry.slab()]
+    pitch_index = {}
+    jobs = []
+    for d in desc:
+        n = max(1, int(round(d["n_primaries"] * scale)))
+        rng = np.random.default_rng([seed, d["job"]])
+        if d["kind"] == "slab":
+            gi = 0
+            pri = primaries.point_beam(n, energy=d["energy"], pixel=(d["job"], 0))
+        else:
+            key = round(d["pitch"], 6)
+            if key not in pitch_index:
+                pitch_index[key] = len(geoms)
+                geoms.append(grating_geometry(pitch=d["pitch"]))
+            gi = pitch_index[key]
+            pri = np.zeros(n, dtype=primaries.PRI_DTYPE)
+            pri["pos"][:, 0] = rng.uniform(-32.0, 32.0, n)
+            pri["pos"][:, 1] = rng.uniform(-32.0, 32.0, n)
+            pri["pos"][:, 2] = GRATING_Z0
+            pri["dir"] = (0.0, 0.0, -1.0)
+            pri["E"] = d["energy"]
+            pri["px"] = d["job"]
+        jobs.append((gi, d["seed"], pri))
+    return geoms, [materials.silicon(e_max), materials.pmma(e_max)], jobs, desc

@@ -1,0 +1,76 @@
+"""Batched persistent runs: per-job results equal those of each job run alone
+in the plain wavefront with the same seed (the random streams are keyed by
+job seed, primary index and ancestry only), for several launch shapes and
+refill thresholds."""
+import os
+
+import numpy as np
+import pytest
+
+import nebula_b200 as nb
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_batch(tmp_path_factory):
+    from nebula_b200.synth import workloads, geometry, materials, nmat
+    d = tmp_path_factory.mktemp("batch")
+    geoms_tri, specs, jobs, desc = workloads.batch(seed=7, n_jobs=8, scale=0.004, e_max=30e3)
+    # keep the test bounded: at most 3 keV
+    jobs = [(gi, seed, pri[:400]) for gi, seed, pri in jobs]
+    for _, _, pri in jobs:
+        pri["E"] = np.minimum(pri["E"], 3000.0)
+    geoms = []
+    for i, t in enumerate(geoms_tri):
+        p = os.path.join(str(d), "g%d.tri" % i)
+        geometry.write_tri(p, t)
+        geoms.append(nb.Geometry.from_tri_file(p))
+    mats = []
+    for sp in specs:
+        p = os.path.join(str(d), sp.name + ".nmat")
+        nmat.write(p, materials.build_raw_material(sp))
+        mats.append(nb.Material.load(p))
+    return geoms, mats, jobs
+
+
+def _plain_yields(geoms, mats, jobs):
+    out = []
+    for gi, seed, pri in jobs:
+        g = geoms[gi]
+        n_mat = 1 if gi == 0 else 2
+        sim = nb.Simulation(g, mats[:n_mat], capacity=1 << 14, seed=seed)
+        sim.push(pri)
+        sim.run()
+        rec = sim.flush_detected()
+        out.append((int((rec["E"] < 50).sum()), int((rec["E"] >= 50).sum())))
+        sim.close()
+    return np.array(out)
+
+
+@pytest.mark.parametrize("block,thr,cap,graph", [(256, 1.0, 1 << 16, True), (512, 0.3, 1 << 14, True),
+                                                 (128, 0.5, 1 << 12, False)])
+def test_batch_per_job_yields_equal_plain_runs(small_batch, block, thr, cap, graph):
+    geoms, mats, jobs = small_batch
+    ref = _plain_yields(geoms, mats, jobs)
+    b = nb.Batch(geoms, mats, capacity=cap, refill_threshold=thr, block_size=block, use_graph=graph)
+    b.set_jobs(jobs)
+    for _ in range(2):      # a second run on the same batch object starts clean
+        b.run()
+        se, bse = b.job_yields()
+        assert np.array_equal(se, ref[:, 0]), (se, ref[:, 0])
+        assert np.array_equal(bse, ref[:, 1])
+        c = b.counters()
+        assert c["primaries_started"] == sum(len(p) for _, _, p in jobs)
+        assert c["primaries_started"] + c["spawned"] == c["detected"] + c["terminated"]
+        assert c["queue_overflow"] == 0
+    b.close()
+
+
+def test_batch_rejects_bad_job_ranges(small_batch):
+    geoms, mats, jobs = small_batch
+    b = nb.Batch(geoms, mats, capacity=1 << 12)
+    bad = [(len(geoms), 1, jobs[0][2])]
+    with pytest.raises(nb.NblError):
+        b.set_jobs(bad)
+    b.close()
