@@ -305,7 +305,9 @@ def main():
         ms = [nb.Material.load(p) for p in mats]
         n_pri = len(w.primaries)
         stream = torch.cuda.Stream(device=dev)
-        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=1000 + rank, device=dev, tally=w.n_pixels,
+        from nebula_b200 import replicas
+        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=replicas.replica_seed(1000, rank), device=dev,
+                            tally=w.n_pixels,
                             stream=stream.cuda_stream, record_capacity=args.record_capacity)
         pri_dev = torch.from_numpy(w.primaries.view(np.uint8)).to(f"cuda:{dev}")
         pri_host = torch.from_numpy(w.primaries.view(np.uint8).copy()).pin_memory()
@@ -352,9 +354,7 @@ def main():
             torch.cuda.synchronize(dev)
         ms = ev0.elapsed_time(ev1)
         if dist:
-            t = torch.tensor([ms], device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = replicas.max_over_ranks(ms, dist, device=f"cuda:{dev}")
 
         # timed: end to end from pinned host records
         h2d = n_pri * 36
@@ -370,9 +370,7 @@ def main():
         torch.cuda.synchronize(dev)
         e2e_ms = e0.elapsed_time(e1)
         if dist:
-            t = torch.tensor([e2e_ms], device=f"cuda:{dev}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+            e2e_ms = replicas.max_over_ranks(e2e_ms, dist, device=f"cuda:{dev}")
 
         value = n_pri * args.steps * world / (ms / 1000.0)
         e2e_value = n_pri * args.steps * world / (e2e_ms / 1000.0)

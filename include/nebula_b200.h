@@ -237,6 +237,27 @@ nbl_status nbl_sim_set_seed(nbl_sim* s, uint64_t seed);
 nbl_status nbl_sim_kernel_ms(nbl_sim* s, double* ms);
 void nbl_sim_destroy(nbl_sim* s);
 
+/* ------------------------------------------------------------ adjoint */
+/* Continuous material parameters theta, 3 per material for up to 2 materials:
+ * theta[3m+0] inelastic inverse-mean-free-path scale, theta[3m+1] elastic
+ * scale (both 1 as loaded), theta[3m+2] work function in eV (barrier minus
+ * Fermi energy as loaded).  No counterpart in the reference (its parameters
+ * are fixed at material load). */
+nbl_status nbl_sim_set_theta(nbl_sim* s, const float* theta, int32_t n);
+nbl_status nbl_sim_get_theta(nbl_sim* s, float* theta, int32_t n);
+/* Score-function (likelihood-ratio) gradients of the per-pixel SE and BSE
+ * counts: a simulation created with params.adjoint = 1 replays each primary
+ * with the same random numbers as an adjoint = 0 run with the same seed
+ * (identical trajectories and tallies) while every electron carries
+ * d log p(path)/d theta -- its own free flights (chosen event and survival
+ * densities) and boundary transmissions, plus its ancestry up to its creation
+ * -- and every detection adds it to its pixel.  Output: FP64 sums,
+ * [tally_ny][tally_nx][6] each; divide by the primaries of a pixel for the
+ * yield gradient.  The work-function derivative is the score of the
+ * transmission probability only: its deterministic effects on the crossing
+ * (energy shift, refraction) are not differentiated. */
+nbl_status nbl_sim_gradients(nbl_sim* s, double* grad_se, double* grad_bse);
+
 /* ------------------------------------------------------------ batched runs */
 /* Many scan jobs -- each with its own geometry, primaries and seed -- fed
  * into one electron pool by a persistent kernel: every wavefront iteration of

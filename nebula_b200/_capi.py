@@ -123,6 +123,9 @@ _DECLS = [
     ("nbl_sim_counters", C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     ("nbl_sim_reset", C.c_int, [C.c_void_p]),
     ("nbl_sim_set_seed", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("nbl_sim_set_theta", C.c_int, [C.c_void_p, f32p, C.c_int32]),
+    ("nbl_sim_get_theta", C.c_int, [C.c_void_p, f32p, C.c_int32]),
+    ("nbl_sim_gradients", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("nbl_sim_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_destroy", None, [C.c_void_p]),
     ("nbl_batch_params_defaults", None, [C.POINTER(BatchParams)]),

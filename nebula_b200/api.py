@@ -296,6 +296,29 @@ class Simulation:
     def set_seed(self, seed):
         check(lib().nbl_sim_set_seed(self._h, seed))
 
+    def n_theta(self):
+        return 3 * min(len(self.materials), 2)
+
+    def set_theta(self, theta):
+        """(inelastic scale, elastic scale, work function) per material."""
+        t = np.ascontiguousarray(theta, np.float32).ravel()
+        check(lib().nbl_sim_set_theta(self._h, _fp(t), len(t)))
+
+    def get_theta(self):
+        t = np.zeros(self.n_theta(), np.float32)
+        check(lib().nbl_sim_get_theta(self._h, _fp(t), len(t)))
+        return t
+
+    def gradients(self):
+        """Per-pixel FP64 sums of d(SE count)/d theta and d(BSE count)/d
+        theta, shape (ny, nx, 6) each (adjoint simulations only)."""
+        nx, ny = self.tally
+        gs = np.zeros((ny, nx, 6), np.float64)
+        gb = np.zeros((ny, nx, 6), np.float64)
+        check(lib().nbl_sim_gradients(self._h, gs.ctypes.data_as(C.POINTER(C.c_double)),
+                                      gb.ctypes.data_as(C.POINTER(C.c_double))))
+        return gs, gb
+
     def reset(self):
         check(lib().nbl_sim_reset(self._h))
 

@@ -791,6 +791,50 @@ nbl_status nbl_sim_reset(nbl_sim* s)
 	});
 }
 
+nbl_status nbl_sim_set_theta(nbl_sim* s, const float* theta, int32_t n)
+{
+	return guard([&] {
+		require(s && theta, "null argument");
+		require(n == 3 * std::min(s->mats.n, 2), "theta holds 3 values per material (at most 2 materials)");
+		set_device(s->device);
+		std::vector<DevMaterial>& h = s->mats.host;
+		for (int m = 0; m < n / 3; ++m) {
+			require(theta[3 * m] > 0 && theta[3 * m + 1] > 0, "mean-free-path scales must be positive");
+			h[m].in_scale = theta[3 * m];
+			h[m].el_scale = theta[3 * m + 1];
+			h[m].barrier = h[m].fermi + theta[3 * m + 2];
+		}
+		CU(cudaMemcpyAsync(s->mats.mats.p, h.data(), h.size() * sizeof(DevMaterial), cudaMemcpyHostToDevice, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+	});
+}
+
+nbl_status nbl_sim_get_theta(nbl_sim* s, float* theta, int32_t n)
+{
+	return guard([&] {
+		require(s && theta, "null argument");
+		require(n == 3 * std::min(s->mats.n, 2), "theta holds 3 values per material (at most 2 materials)");
+		const std::vector<DevMaterial>& h = s->mats.host;
+		for (int m = 0; m < n / 3; ++m) {
+			theta[3 * m] = h[m].in_scale;
+			theta[3 * m + 1] = h[m].el_scale;
+			theta[3 * m + 2] = h[m].barrier - h[m].fermi;
+		}
+	});
+}
+
+nbl_status nbl_sim_gradients(nbl_sim* s, double* grad_se, double* grad_bse)
+{
+	return guard([&] {
+		require(s && grad_se && grad_bse, "null argument");
+		require(s->params.adjoint && s->grad_se.p, "gradients need adjoint = 1 and a tally grid");
+		set_device(s->device);
+		CU(cudaMemcpyAsync(grad_se, s->grad_se.p, s->grad_se.bytes, cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaMemcpyAsync(grad_bse, s->grad_bse.p, s->grad_bse.bytes, cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+	});
+}
+
 nbl_status nbl_sim_set_seed(nbl_sim* s, uint64_t seed)
 {
 	return guard([&] {

@@ -102,6 +102,7 @@ struct DeviceGeometry {
 struct DeviceMaterials {
 	DevBuf tables, mats;
 	int n = 0;
+	std::vector<DevMaterial> host;   // the device array's contents
 	void upload(const std::vector<const HostMaterial*>& ms, cudaStream_t s)
 	{
 		n = (int)ms.size();
@@ -142,6 +143,7 @@ struct DeviceMaterials {
 		mats.alloc(std::max<size_t>(dm.size(), 1) * sizeof(DevMaterial));
 		CU(cudaMemcpyAsync(mats.p, dm.data(), dm.size() * sizeof(DevMaterial), cudaMemcpyHostToDevice, s));
 		CU(cudaStreamSynchronize(s));
+		host = dm;
 	}
 };
 
