@@ -100,19 +100,26 @@ typedef struct nbl_table {
 	const float* data;
 } nbl_table;
 
-/* Tables and constants of one material after full_penn::create and
- * kieft_elastic::create:
+/* Tables and constants of one material after the reference's create()
+ * transforms (full_penn::create, kieft_inelastic::create, kieft_elastic::create):
  *   el_imfp   log(elastic 1/lambda / nm^-1)      over log(E/eV)
  *   el_icdf   cos(theta)                          over log(E/eV) x P
+ * Full-Penn inelastic model (full_penn.h:294-406; present when models & 1):
  *   in_imfp   log(inelastic 1/lambda / nm^-1)    over log(E/eV)
  *   in_omega  log(omega/eV)                       over log(E/eV) x P
  *   in_q      hbar q / sqrt(2m) in eV^1/2         over log(E/eV) x omega/E x P
  *   in_binding binding energy in eV, -1 = none    over log(E/eV) x log(omega/E) x P
+ * Kieft-Bosch inelastic model (kieft/inelastic.h:215-331; present when models & 2):
+ *   ki_imfp   log(inelastic 1/lambda / nm^-1)    over log(E/eV)
+ *   ki_w0     log(omega'/eV) zero-momentum loss   over log(E/eV) x P
+ *   ki_binding binding energy in eV, -1 = none    over log(E/eV) x P (get_rounddown)
  * barrier = fermi + work function (eV); band_gap -1 for metals;
  * recoil_const = 4 m_e / M (elastic.h:161-163). */
 typedef struct nbl_material_tables {
 	nbl_table el_imfp, el_icdf, in_imfp, in_omega, in_q, in_binding;
 	float fermi, band_gap, barrier, phonon_loss, recoil_const;
+	int32_t models;              /* bit 0: Full-Penn tables, bit 1: Kieft-Bosch tables */
+	nbl_table ki_imfp, ki_w0, ki_binding;
 } nbl_material_tables;
 
 typedef struct nbl_material nbl_material;
@@ -158,16 +165,22 @@ nbl_status nbl_ray_query(const nbl_geometry* g, int device, int64_t n, const flo
 	const float* dist, const int32_t* ignore_tri, const int32_t* ignore_mat, float* out_dist, int32_t* out_tri);
 
 /* ------------------------------------------------------------ physics */
-/* Physics options, mirroring physics_config.h:20-46.  The build compiles the
- * reference's default selection; other values are rejected. */
+/* Physics selection, mirroring physics_config.h:20-46 and the option bools of
+ * the models it names (full_penn.h:15-19, kieft/inelastic.h:12-23,
+ * kieft/elastic.h:17-22, boundary_intersect.h:11-19).  The reference picks
+ * these at compile time; here they are run-time values of one build.  Each
+ * flag is 0 or 1; nbl_physics_defaults sets the reference's selection. */
 typedef struct nbl_physics_opts {
-	int32_t inelastic_model;        /* 0: Full Penn (the only one built) */
-	int32_t generate_secondaries;   /* 1 */
-	int32_t acoustic_phonon_loss;   /* 1 */
-	int32_t atomic_recoil_loss;     /* 1 */
-	int32_t quantum_transmission;   /* 1 */
-	int32_t interface_refraction;   /* 1 */
-	int32_t interface_absorption;   /* 0 */
+	int32_t inelastic_model;        /* 0: Full Penn (default), 1: Kieft-Bosch */
+	int32_t generate_secondaries;   /* 1  (both inelastic models) */
+	int32_t acoustic_phonon_loss;   /* 1  elastic */
+	int32_t atomic_recoil_loss;     /* 1  elastic */
+	int32_t quantum_transmission;   /* 1  boundary */
+	int32_t interface_refraction;   /* 1  boundary */
+	int32_t interface_absorption;   /* 0  boundary (Kieft-Bosch empirical absorption) */
+	int32_t optical_phonon_loss;    /* 1  Kieft-Bosch inelastic only */
+	int32_t instantaneous_momentum; /* 1  Kieft-Bosch inelastic only */
+	int32_t momentum_conservation;  /* 1  Kieft-Bosch inelastic only */
 } nbl_physics_opts;
 void nbl_physics_defaults(nbl_physics_opts* o);
 
@@ -286,6 +299,7 @@ typedef struct nbl_batch_params {
 	uint32_t max_iterations;   /* iteration bound of one launch; 0: 1 << 20 */
 	int32_t use_graph;         /* capture the launch in a CUDA graph; 0: plain launch */
 	void* stream;              /* NULL: a library-owned stream */
+	nbl_physics_opts physics;  /* one selection for every job */
 } nbl_batch_params;
 void nbl_batch_params_defaults(nbl_batch_params* p);
 
@@ -333,14 +347,15 @@ nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const* materials
 
 /* ------------------------------------------------------------ debug entry points */
 /* Table lookups on the device (which: 0 el_imfp 1 el_icdf 2 in_imfp 3 in_omega
- * 4 in_q 5 in_binding) for n points; `rounddown` selects get_rounddown. */
+ * 4 in_q 5 in_binding 6 ki_imfp 7 ki_w0 8 ki_binding) for n points;
+ * `rounddown` selects get_rounddown. */
 nbl_status nbl_debug_table_lookup(const nbl_material* m, int device, int32_t which, int32_t rounddown,
 	int64_t n, const float* x, const float* y, const float* z, float* out);
 /* One event per case on the device with caller-supplied uniforms (n_uniforms
  * per case).  kind 1 inelastic, 2 elastic, 3 boundary crossing of triangle
  * tri[i] (geometry g).  state: 7 floats (pos, dir, E) in, out. */
 nbl_status nbl_debug_event(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
-	int device, int32_t kind, int64_t n, const float* state_in, const int32_t* mat_in, const int32_t* tri,
+	int device, const nbl_physics_opts* physics /* NULL: defaults */, int32_t kind, int64_t n, const float* state_in, const int32_t* mat_in, const int32_t* tri,
 	const float* uniforms, int32_t n_uniforms, float* state_out, int32_t* mat_out, int32_t* status,
 	float* se_out, int32_t* has_se, int32_t* used);
 

@@ -45,18 +45,23 @@ class Table(C.Structure):
 
 
 TABLE_NAMES = ("el_imfp", "el_icdf", "in_imfp", "in_omega", "in_q", "in_binding")
+KIEFT_TABLE_NAMES = ("ki_imfp", "ki_w0", "ki_binding")
 
 
 class MaterialTables(C.Structure):
     _fields_ = [(n, Table) for n in TABLE_NAMES] + [
         ("fermi", C.c_float), ("band_gap", C.c_float), ("barrier", C.c_float),
-        ("phonon_loss", C.c_float), ("recoil_const", C.c_float)]
+        ("phonon_loss", C.c_float), ("recoil_const", C.c_float), ("models", C.c_int32)] + [
+        (n, Table) for n in KIEFT_TABLE_NAMES]
+
+
+PHYSICS_OPTION_NAMES = ("inelastic_model", "generate_secondaries", "acoustic_phonon_loss", "atomic_recoil_loss",
+                        "quantum_transmission", "interface_refraction", "interface_absorption",
+                        "optical_phonon_loss", "instantaneous_momentum", "momentum_conservation")
 
 
 class PhysicsOpts(C.Structure):
-    _fields_ = [(n, C.c_int32) for n in (
-        "inelastic_model", "generate_secondaries", "acoustic_phonon_loss", "atomic_recoil_loss",
-        "quantum_transmission", "interface_refraction", "interface_absorption")]
+    _fields_ = [(n, C.c_int32) for n in PHYSICS_OPTION_NAMES]
 
 
 class Params(C.Structure):
@@ -77,7 +82,7 @@ class BatchParams(C.Structure):
     _fields_ = [("device", C.c_int32), ("capacity", C.c_uint32), ("refill_threshold", C.c_float),
                 ("block_size", C.c_uint32), ("queue_factor", C.c_uint32), ("energy_threshold", C.c_float),
                 ("max_events", C.c_uint32), ("max_iterations", C.c_uint32), ("use_graph", C.c_int32),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("physics", PhysicsOpts)]
 
 
 COUNTER_NAMES = ("flights", "boundary", "elastic", "inelastic", "spawned", "detected", "terminated",
@@ -142,7 +147,8 @@ _DECLS = [
                                   C.POINTER(Counters)]),
     ("nbl_debug_table_lookup", C.c_int, [C.c_void_p, C.c_int, C.c_int32, C.c_int32, C.c_int64, f32p, f32p, f32p,
                                          f32p]),
-    ("nbl_debug_event", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.c_int, C.c_int32, C.c_int64,
+    ("nbl_debug_event", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int32, C.c_int, C.POINTER(PhysicsOpts),
+                                  C.c_int32, C.c_int64,
                                   f32p, i32p, i32p, f32p, C.c_int32, f32p, i32p, i32p, f32p, i32p, i32p]),
 ]
 

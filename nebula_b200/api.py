@@ -141,10 +141,18 @@ class Material:
         return cls(h)
 
     def tables(self):
+        """Tables in the transformed domain, by name, as (data, scale) pairs,
+        plus "constants" and "models" (bit 0 Full Penn, bit 1 Kieft-Bosch).
+        Only the tables of the models the material carries are returned."""
         t = _capi.MaterialTables()
         check(lib().nbl_material_get_tables(self._h, C.byref(t)))
-        out = {}
-        for name in _capi.TABLE_NAMES:
+        out = {"models": int(t.models)}
+        names = list(_capi.TABLE_NAMES[:2])
+        if t.models & 1:
+            names += list(_capi.TABLE_NAMES[2:])
+        if t.models & 2:
+            names += list(_capi.KIEFT_TABLE_NAMES)
+        for name in names:
             tb = getattr(t, name)
             n = tb.nx * tb.ny * tb.nz
             data = np.ctypeslib.as_array(tb.data, shape=(n,)).copy().reshape(tb.nx, tb.ny, tb.nz)
@@ -159,7 +167,8 @@ class Material:
         return float(v[0])
 
     def table_lookup(self, which, x, y=None, z=None, rounddown=False, device=0):
-        which = _capi.TABLE_NAMES.index(which) if isinstance(which, str) else which
+        if isinstance(which, str):
+            which = (_capi.TABLE_NAMES + _capi.KIEFT_TABLE_NAMES).index(which)
         x = np.ascontiguousarray(x, np.float32)
         n = len(x)
         y = np.ascontiguousarray(np.zeros(n) if y is None else y, np.float32)
@@ -180,9 +189,23 @@ class Material:
             pass
 
 
-def debug_events(kind, materials, states, mats, uniforms, geometry=None, tris=None, device=0):
+def physics_options(physics=None):
+    """``nbl_physics_opts`` from the reference defaults (physics_config.h)
+    with the entries of the dict ``physics`` overriding them, e.g.
+    ``{"inelastic_model": 1, "interface_refraction": 0}``."""
+    o = _capi.PhysicsOpts()
+    lib().nbl_physics_defaults(C.byref(o))
+    for k, v in (physics or {}).items():
+        if k not in _capi.PHYSICS_OPTION_NAMES:
+            raise KeyError("unknown physics option %r" % k)
+        setattr(o, k, int(v))
+    return o
+
+
+def debug_events(kind, materials, states, mats, uniforms, geometry=None, tris=None, device=0, physics=None):
     """Run one event per case on the device with given uniforms.
     Returns (state_out, material_out, status, se_state, has_se, uniforms_used)."""
+    ph = physics_options(physics)
     states = np.ascontiguousarray(states, np.float32).reshape(-1, 7)
     n = len(states)
     mats_in = np.ascontiguousarray(mats, np.int32)
@@ -195,7 +218,8 @@ def debug_events(kind, materials, states, mats, uniforms, geometry=None, tris=No
     se = np.empty_like(states)
     hs = np.empty(n, np.int32)
     us = np.empty(n, np.int32)
-    check(lib().nbl_debug_event(geometry._h if geometry is not None else None, arr, len(materials), device, kind, n,
+    check(lib().nbl_debug_event(geometry._h if geometry is not None else None, arr, len(materials), device,
+                                C.byref(ph), kind, n,
                                 _fp(states), _ip(mats_in), _ip(tri) if tri is not None else None, _fp(uniforms),
                                 uniforms.shape[1], _fp(so), _ip(mo), _ip(st), _fp(se), _ip(hs), _ip(us)))
     return so, mo, st, se, hs, us
@@ -206,9 +230,10 @@ class Simulation:
 
     def __init__(self, geometry, materials, capacity=1 << 20, seed=0x78C7E39B, energy_threshold=0.0, device=0,
                  tally=(0, 0), hist_bins=200, hist_emax=1000.0, record_capacity=0, block_size=0, grid_size=0,
-                 iterations_per_graph=0, max_events=0, adjoint=False, stream=None):
+                 iterations_per_graph=0, max_events=0, adjoint=False, stream=None, physics=None):
         p = _capi.Params()
         lib().nbl_params_defaults(C.byref(p))
+        p.physics = physics_options(physics)
         p.device = device
         p.capacity = capacity
         p.seed = seed
@@ -341,9 +366,11 @@ class Batch:
     results equal the plain run's."""
 
     def __init__(self, geometries, materials, capacity=1 << 20, refill_threshold=1.0, block_size=256,
-                 queue_factor=4, device=0, use_graph=True, energy_threshold=0.0, max_events=0, stream=None):
+                 queue_factor=4, device=0, use_graph=True, energy_threshold=0.0, max_events=0, stream=None,
+                 physics=None):
         p = _capi.BatchParams()
         lib().nbl_batch_params_defaults(C.byref(p))
+        p.physics = physics_options(physics)
         p.device = device
         p.capacity = capacity
         p.refill_threshold = refill_threshold

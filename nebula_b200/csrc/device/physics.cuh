@@ -5,9 +5,11 @@
 // order and its random-draw order, so that given the same uniforms the GPU
 // and the reference CPU build differ only by the last-ulp differences of the
 // transcendental functions (logf, expf, sinf/cosf, atan2f, cbrtf):
-//   * kieft_elastic<gpu,true,true>::execute  (physics/kieft/elastic.h:67-115)
-//   * full_penn<gpu,true>::execute           (physics/full_penn.h:62-288)
-//   * boundary_intersect<true,true,false>::execute (physics/boundary_intersect.h:38-155)
+//   * kieft_elastic<gpu,phonon,recoil>::execute    (physics/kieft/elastic.h:67-115)
+//   * full_penn<gpu,gen_se>::execute               (physics/full_penn.h:62-288)
+//   * kieft_inelastic<gpu,opl,gen_se,im,mc>::execute (physics/kieft/inelastic.h:63-209)
+//   * boundary_intersect<qt,refraction,absorption>::execute (physics/boundary_intersect.h:38-155)
+//   with the option bools taken from a run-time word of PH_* bits.
 //   * free-path sampling: scatter_list::sample_path visits the processes with
 //     tuple::for_each, which runs last-to-first (core/scatter_list.h:101-107,
 //     common/tuple.h:113-118), so the elastic path is drawn before the
@@ -97,8 +99,10 @@ template<class R> __device__ __forceinline__ float sample_path(const DevTable& i
 	return fm(-tau, __logf(rng.unit()));
 }
 
-// Elastic event (elastic.h:67-115) with acoustic-phonon and atomic-recoil loss.
-template<class R> __device__ __forceinline__ void elastic_event(const DevMaterial& m, Electron& p, R& rng)
+// Elastic event (elastic.h:67-115), acoustic-phonon and atomic-recoil loss
+// as selected.
+template<class R> __device__ __forceinline__ void elastic_event(const DevMaterial& m, Electron& p, R& rng,
+	uint32_t ph = PH_DEFAULT)
 {
 	const float x = __logf(p.E);
 	const float y = rng.unit();
@@ -107,17 +111,20 @@ template<class R> __device__ __forceinline__ void elastic_event(const DevMateria
 	p.dir = vnormalised(p.dir);
 	const V3 normal_dir = vnormalised(make_normal_vec(p.dir, draw_phi(rng)));
 	p.dir = vadd(vmul(p.dir, cos_theta), vmul(normal_dir, sin_theta));
-	if (p.E < 200.0f)
-		p.E = fs(p.E, smin(50e-3f, m.phonon_loss));
-	else
+	if (p.E < 200.0f) {
+		if (ph & PH_PHONON)
+			p.E = fs(p.E, smin(50e-3f, m.phonon_loss));
+	} else if (ph & PH_RECOIL) {
 		p.E = fs(p.E, fm(fm(m.recoil_const, fs(1.0f, cos_theta)), p.E));
+	}
 }
 
 // Inelastic event (full_penn.h:62-288).  Returns true and fills `se` when a
 // secondary electron is created.  The plasmon-decay rejection loop is capped
 // at 64 trials (the last trial is kept); the reference loop is unbounded but
 // its acceptance rate is above one half.
-template<class R> __device__ __forceinline__ bool inelastic_event(const DevMaterial& m, Electron& p, Electron& se, R& rng)
+template<class R> __device__ __forceinline__ bool penn_event(const DevMaterial& m, Electron& p, Electron& se, R& rng,
+	uint32_t ph)
 {
 	float omega;
 	{
@@ -155,6 +162,8 @@ template<class R> __device__ __forceinline__ bool inelastic_event(const DevMater
 			const float s2 = __fsqrt_rn(fs(1.0f, fm(c2, c2)));
 			p.E = fs(p.E, omega);
 			p.dir = vadd(vmul(p.dir, c2), vmul(prim_normal_dir, s2));
+			if (!(ph & PH_GEN_SE))
+				return false;
 
 			se.pos = p.pos;
 			const float k_fermi = __fsqrt_rn(m.fermi);
@@ -218,18 +227,101 @@ template<class R> __device__ __forceinline__ bool inelastic_event(const DevMater
 	se.dir = sdir;
 	p.E = fs(p.E, omega);
 	p.dir = vsub(p.dir, smul(cos_theta, sdir));
-	return true;
+	return (ph & PH_GEN_SE) != 0;
+}
+
+// Kieft-Bosch inelastic event (kieft/inelastic.h:63-209): zero-momentum loss
+// omega' from its ICDF, a binding energy from the ionisation ICDF (rounddown),
+// the total loss omega from Ashley's distribution between the kinematic
+// limits, Ivanchenko angles for the secondary.  The two logarithms and the
+// expm1 of the omega draw take arguments close to 1 and 0, so they use the
+// accurate library functions rather than the SFU forms.
+template<class R> __device__ __forceinline__ bool kieft_event(const DevMaterial& m, Electron& p, Electron& se, R& rng,
+	uint32_t ph)
+{
+	float omega0;
+	{
+		const float x = __logf(p.E);
+		const float y = rng.unit();
+		omega0 = __expf(table2_get(m.in_omega, x, y));
+	}
+	float binding;
+	{
+		const float x = __logf(omega0);
+		const float y = rng.unit();
+		binding = table2_rounddown(m.in_binding, x, y);
+	}
+	float omega;
+	{
+		const float omega_max = fm(0.5f, fs(fa(p.E, omega0), m.fermi));
+		float omega_min = omega0;
+		float w0 = smin(fs(omega0, 1.0f), fs(smax(0.0f, binding), m.fermi));
+		if (p.E > fm(2.0f, omega0)) {
+			omega_min = fm(0.5f, fs(fa(p.E, omega0), __fsqrt_rn(fm(p.E, fs(p.E, fm(2.0f, omega0))))));
+			w0 = omega0;
+		}
+		const float U = rng.unit();
+		if ((w0 > 0.0f) && (omega_min > w0) && (omega_min < omega_max)) {
+			const float f_min = fm(fd(1.0f, w0), logf(fd(fs(omega_min, w0), omega_min)));
+			const float f_max = fm(fd(1.0f, w0), logf(fd(fs(omega_max, w0), omega_max)));
+			omega = fd(-w0, expm1f(fm(w0, fa(fm(f_min, fs(1.0f, U)), fm(f_max, U)))));
+		} else {
+			omega = fd(fm(omega0, omega_max), fa(fm(omega0, fs(1.0f, U)), fm(omega_max, U)));
+		}
+	}
+	if (binding < 0.0f) {
+		if (m.band_gap < 0.0f) {
+			// metals: the reference leaves the Fermi-sea excitation open
+		} else if (omega0 > m.band_gap) {
+			binding = m.band_gap;
+		} else {
+			if (ph & PH_OPT_PHONON)
+				p.E = fs(p.E, omega0);
+			return false;
+		}
+	}
+	binding = smax(0.0f, binding);
+	p.dir = vnormalised(p.dir);
+	const V3 normal_dir = vnormalised(make_normal_vec(p.dir, draw_phi(rng)));
+	const float K = fa(fs(p.E, m.fermi), fm(2.0f, binding));
+	const float dK = fa(binding, omega);
+	const float cos_theta = __fsqrt_rn(fd(dK, K));
+	const float sin_theta = __fsqrt_rn(fs(1.0f, clampf(fm(cos_theta, cos_theta), 0.0f, 1.0f)));
+	V3 sdir = vadd(vmul(p.dir, cos_theta), vmul(normal_dir, sin_theta));
+	if (ph & PH_INST_MOM) {
+		sdir = vnormalised(sdir);
+		sdir = vadd(sdir, smul(__fsqrt_rn(fd(binding, dK)), uniform_vector(rng)));
+	}
+	sdir = vnormalised(sdir);
+	se.E = fs(fa(m.fermi, omega), binding);
+	se.pos = p.pos;
+	se.dir = sdir;
+	p.E = fs(p.E, omega);
+	if (ph & PH_MOM_CONS)
+		p.dir = vsub(p.dir, smul(cos_theta, sdir));
+	return (ph & PH_GEN_SE) != 0;
+}
+
+// Inelastic event of the selected model.  Returns true and fills `se` when a
+// secondary electron is created.
+template<class R> __device__ __forceinline__ bool inelastic_event(const DevMaterial& m, Electron& p, Electron& se, R& rng,
+	uint32_t ph = PH_DEFAULT)
+{
+	if (ph & PH_KIEFT)
+		return kieft_event(m, p, se, rng, ph);
+	return penn_event(m, p, se, rng, ph);
 }
 
 enum : int { ST_RUNNING = 0, ST_DETECTED = 1, ST_TERMINATED = 2 };
 
-// Boundary crossing (boundary_intersect.h:38-155): quantum transmission and
-// refraction on, empirical absorption off.  `score_w` (optional) receives
-// d log P(outcome) / d barrier_out and d / d barrier_in for the adjoint.
+// Boundary crossing (boundary_intersect.h:38-155) with quantum transmission,
+// refraction and the Kieft-Bosch empirical absorption as selected.  `score`
+// (optional) receives d log P(outcome) / d barrier_out and d / d barrier_in
+// for the adjoint.
 struct BoundaryScore { float d_in, d_out; int mat_in, mat_out; };
 
 template<class R> __device__ __forceinline__ int boundary_event(const DevTriangle& T, const DevMaterial* __restrict__ mats,
-	Electron& p, int& material, R& rng, BoundaryScore* score = nullptr)
+	Electron& p, int& material, R& rng, BoundaryScore* score = nullptr, uint32_t ph = PH_DEFAULT)
 {
 	const V3 nd = vnormalised(p.dir);
 	const V3 n = vnormalised(v3(T.nx, T.ny, T.nz));
@@ -250,27 +342,40 @@ template<class R> __device__ __forceinline__ int boundary_event(const DevTriangl
 	if (min_ >= 0) dU = fs(dU, mats[min_].barrier);
 	if (mout >= 0) dU = fa(dU, mats[mout].barrier);
 	const float Ec2 = fm(fm(p.E, c), c);
+	float g = 0.0f;                                          // d log P(outcome) / d dU
 	if (fa(Ec2, dU) > 0.0f) {
 		const float s = __fsqrt_rn(fa(1.0f, fd(dU, Ec2)));
-		const float Tr = fd(fm(4.0f, s), fm(fa(1.0f, s), fa(1.0f, s)));
+		const bool qt = (ph & PH_QT) != 0;
+		const float Tr = qt ? fd(fm(4.0f, s), fm(fa(1.0f, s), fa(1.0f, s))) : 1.0f;
 		const bool transmit = rng.unit() < Tr;
-		if (score) {
+		if (score && qt) {
 			// T(s) = 4s/(1+s)^2, s^2 = 1 + dU/(E c^2):
 			// dlogT/ddU = (1-s)/(s(1+s)) * ds/ddU, ds/ddU = 1/(2 s E c^2)
 			const float dlogT_ds = fd(fs(1.0f, s), fm(s, fa(1.0f, s)));
 			const float ds_ddU = fd(1.0f, fm(fm(2.0f, s), Ec2));
-			float g = fm(dlogT_ds, ds_ddU);                 // d log T / d dU
-			if (!transmit) g = fm(-g, fd(Tr, fs(1.0f, Tr))); // d log(1-T) / d dU
-			score->d_out = g;                                // dU = +barrier_out
-			score->d_in = -g;                                //      -barrier_in
+			g = fm(dlogT_ds, ds_ddU);                         // d log T / d dU
+			if (!transmit) g = fm(-g, fd(Tr, fs(1.0f, Tr)));  // d log(1-T) / d dU
 		}
 		if (transmit) {
-			p.dir = vadd(vsub(nd, vmul(n, c)), vmul(smul(s, n), c));
+			if (ph & PH_REFRACT)
+				p.dir = vadd(vsub(nd, vmul(n, c)), vmul(smul(s, n), c));
 			p.E = fa(p.E, dU);
 			material = mout;
+			if (score) { score->d_out = g; score->d_in = -g; }   // dU = +barrier_out - barrier_in
 			return ST_RUNNING;
 		}
 	}
+	if ((ph & PH_ABSORB) && dU < 0.0f) {
+		// empirical absorption with probability exp(1 + E / (2 dU))
+		const float pa = expf(fa(1.0f, fd(fm(0.5f, p.E), dU)));
+		if (rng.unit() < pa)
+			return ST_TERMINATED;
+		if (score) {
+			// d log(1 - pa) / d dU = pa / (1 - pa) * E / (2 dU^2)
+			g = fa(g, fm(fd(pa, fs(1.0f, pa)), fd(fm(0.5f, p.E), fm(dU, dU))));
+		}
+	}
+	if (score) { score->d_out = g; score->d_in = -g; }
 	p.dir = vsub(nd, vmul(smul(2.0f, n), c));
 	return ST_RUNNING;
 }

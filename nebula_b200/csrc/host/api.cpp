@@ -19,6 +19,22 @@ namespace nbl {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& m) { g_last_error = m; }
 
+uint32_t physics_bits(const nbl_physics_opts& o)
+{
+	const int32_t flags[9] = { o.generate_secondaries, o.acoustic_phonon_loss, o.atomic_recoil_loss,
+		o.quantum_transmission, o.interface_refraction, o.interface_absorption, o.optical_phonon_loss,
+		o.instantaneous_momentum, o.momentum_conservation };
+	const uint32_t bits[9] = { PH_GEN_SE, PH_PHONON, PH_RECOIL, PH_QT, PH_REFRACT, PH_ABSORB, PH_OPT_PHONON,
+		PH_INST_MOM, PH_MOM_CONS };
+	require(o.inelastic_model == 0 || o.inelastic_model == 1, "inelastic_model must be 0 (Full Penn) or 1 (Kieft-Bosch)");
+	uint32_t r = o.inelastic_model == 1 ? PH_KIEFT : 0u;
+	for (int i = 0; i < 9; ++i) {
+		require(flags[i] == 0 || flags[i] == 1, "physics options are 0 or 1");
+		if (flags[i]) r |= bits[i];
+	}
+	return r;
+}
+
 namespace {
 
 void check_table(const nbl_table& t, int rank, const char* name)
@@ -304,13 +320,23 @@ nbl_status nbl_material_create(const nbl_material_tables* t, nbl_material** out)
 {
 	return guard([&] {
 		require(t && out, "null argument");
+		require(t->models >= 1 && t->models <= 3, "models must name the Full-Penn (1) and/or Kieft-Bosch (2) tables");
 		check_table(t->el_imfp, 1, "el_imfp"); check_table(t->el_icdf, 2, "el_icdf");
-		check_table(t->in_imfp, 1, "in_imfp"); check_table(t->in_omega, 2, "in_omega");
-		check_table(t->in_q, 3, "in_q"); check_table(t->in_binding, 3, "in_binding");
 		auto m = std::make_unique<nbl_material>();
 		m->m.el_imfp = copy_table(t->el_imfp); m->m.el_icdf = copy_table(t->el_icdf);
-		m->m.in_imfp = copy_table(t->in_imfp); m->m.in_omega = copy_table(t->in_omega);
-		m->m.in_q = copy_table(t->in_q); m->m.in_binding = copy_table(t->in_binding);
+		if (t->models & 1) {
+			check_table(t->in_imfp, 1, "in_imfp"); check_table(t->in_omega, 2, "in_omega");
+			check_table(t->in_q, 3, "in_q"); check_table(t->in_binding, 3, "in_binding");
+			m->m.in_imfp = copy_table(t->in_imfp); m->m.in_omega = copy_table(t->in_omega);
+			m->m.in_q = copy_table(t->in_q); m->m.in_binding = copy_table(t->in_binding);
+		}
+		if (t->models & 2) {
+			check_table(t->ki_imfp, 1, "ki_imfp"); check_table(t->ki_w0, 2, "ki_w0");
+			check_table(t->ki_binding, 2, "ki_binding");
+			m->m.ki_imfp = copy_table(t->ki_imfp); m->m.ki_w0 = copy_table(t->ki_w0);
+			m->m.ki_binding = copy_table(t->ki_binding);
+		}
+		m->m.models = t->models;
 		m->m.fermi = t->fermi; m->m.band_gap = t->band_gap; m->m.barrier = t->barrier;
 		m->m.phonon_loss = t->phonon_loss; m->m.recoil_const = t->recoil_const;
 		*out = m.release();
@@ -326,6 +352,8 @@ nbl_status nbl_material_get_tables(const nbl_material* m, nbl_material_tables* o
 		out->in_q = m->m.in_q.view(); out->in_binding = m->m.in_binding.view();
 		out->fermi = m->m.fermi; out->band_gap = m->m.band_gap; out->barrier = m->m.barrier;
 		out->phonon_loss = m->m.phonon_loss; out->recoil_const = m->m.recoil_const;
+		out->models = m->m.models;
+		out->ki_imfp = m->m.ki_imfp.view(); out->ki_w0 = m->m.ki_w0.view(); out->ki_binding = m->m.ki_binding.view();
 	});
 }
 
@@ -335,7 +363,11 @@ nbl_status nbl_material_max_energy(const nbl_material* m, float* out)
 		require(m && out, "null argument");
 		// get_max_energy: exp of the last IMFP abscissa (full_penn.h:42-45, elastic.h:46-49)
 		auto emax = [](const HostTable& t) { return std::exp(t.x_min + (t.nx - 1) / t.x_step); };
-		*out = std::min(emax(m->m.in_imfp), emax(m->m.el_imfp));
+		// (over the inelastic tables of every model the material carries)
+		float e = emax(m->m.el_imfp);
+		if (m->m.models & 1) e = std::min(e, emax(m->m.in_imfp));
+		if (m->m.models & 2) e = std::min(e, emax(m->m.ki_imfp));
+		*out = e;
 	});
 }
 
@@ -487,6 +519,9 @@ void nbl_physics_defaults(nbl_physics_opts* o)
 	o->quantum_transmission = 1;
 	o->interface_refraction = 1;
 	o->interface_absorption = 0;
+	o->optical_phonon_loss = 1;
+	o->instantaneous_momentum = 1;
+	o->momentum_conservation = 1;
 }
 
 void nbl_params_defaults(nbl_params* p)
@@ -503,11 +538,7 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 	return guard([&] {
 		require(g && materials && params && out, "null argument");
 		require(n_materials >= 1 && n_materials <= 127, "need 1..127 materials");
-		const nbl_physics_opts& ph = params->physics;
-		require(ph.inelastic_model == 0 && ph.generate_secondaries == 1 && ph.acoustic_phonon_loss == 1 &&
-			ph.atomic_recoil_loss == 1 && ph.quantum_transmission == 1 && ph.interface_refraction == 1 &&
-			ph.interface_absorption == 0,
-			"only the reference's default physics selection (physics_config.h) is built");
+		const uint32_t phys = physics_bits(params->physics);
 		int max_mat = -1;
 		for (const nbl_triangle& t : g->g.tris)
 			max_mat = std::max(max_mat, std::max(t.material_in, t.material_out));
@@ -544,7 +575,7 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 			require(materials[i] != nullptr, "null material");
 			ms.push_back(&materials[i]->m);
 		}
-		s->mats.upload(ms, s->stream);
+		s->mats.upload(ms, s->stream, phys);
 
 		StepParams& sp = s->sp;
 		sp.geom = s->geom.view;
@@ -563,6 +594,7 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		// ramps up while the cascades of the first primaries develop
 		sp.ramp = std::max<uint32_t>(cap / 16, 256);
 		sp.refill_below = cap;
+		sp.phys = phys;
 		const bool adj = params->adjoint != 0;
 		for (int b = 0; b < 2; ++b)
 			for (int q = 0; q < N_QUEUES; ++q) {
@@ -868,14 +900,17 @@ nbl_status nbl_debug_table_lookup(const nbl_material* m, int device, int32_t whi
 {
 	return guard([&] {
 		require(m && x && y && z && out, "null argument");
-		require(which >= 0 && which <= 5 && n >= 0, "bad arguments");
+		require(which >= 0 && which <= 8 && n >= 0, "bad arguments");
+		// 6..8: the Kieft-Bosch tables, uploaded in the inelastic slots
+		// (ki_imfp -> in_imfp, ki_w0 -> in_omega, ki_binding -> in_binding, 2-D)
+		const bool kieft = which >= 6;
 		set_device(device);
 		if (n == 0) return;
 		cudaStream_t s;
 		CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
 		struct S { cudaStream_t s; ~S() { cudaStreamDestroy(s); } } sg{ s };
 		DeviceMaterials dm;
-		dm.upload({ &m->m }, s);
+		dm.upload({ &m->m }, s, kieft ? (PH_DEFAULT | PH_KIEFT) : PH_DEFAULT);
 		DevBuf b(n * 16);
 		float* dx = b.as<float>();
 		float* dy = dx + n;
@@ -891,7 +926,7 @@ nbl_status nbl_debug_table_lookup(const nbl_material* m, int device, int32_t whi
 }
 
 nbl_status nbl_debug_event(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials, int device,
-	int32_t kind, int64_t n, const float* state_in, const int32_t* mat_in, const int32_t* tri, const float* uniforms,
+	const nbl_physics_opts* physics, int32_t kind, int64_t n, const float* state_in, const int32_t* mat_in, const int32_t* tri, const float* uniforms,
 	int32_t n_uniforms, float* state_out, int32_t* mat_out, int32_t* status, float* se_out, int32_t* has_se,
 	int32_t* used)
 {
@@ -907,6 +942,9 @@ nbl_status nbl_debug_event(const nbl_geometry* g, nbl_material* const* materials
 			for (int64_t i = 0; i < n; ++i)
 				require(mat_in[i] >= 0 && mat_in[i] < n_materials, "scatter events need a physical material");
 		}
+		nbl_physics_opts def;
+		nbl_physics_defaults(&def);
+		const uint32_t phys = physics_bits(physics ? *physics : def);
 		set_device(device);
 		if (n == 0) return;
 		cudaStream_t s;
@@ -915,7 +953,7 @@ nbl_status nbl_debug_event(const nbl_geometry* g, nbl_material* const* materials
 		std::vector<const HostMaterial*> ms;
 		for (int i = 0; i < n_materials; ++i) ms.push_back(&materials[i]->m);
 		DeviceMaterials dm;
-		dm.upload(ms, s);
+		dm.upload(ms, s, phys);
 		DeviceGeometry dg;
 		if (g) dg.upload(g->g, s);
 		const size_t nu = (size_t)n * n_uniforms;
@@ -936,7 +974,7 @@ nbl_status nbl_debug_event(const nbl_geometry* g, nbl_material* const* materials
 		if (tri) CU(cudaMemcpyAsync(d_tri, tri, n * 4, cudaMemcpyHostToDevice, s));
 		else CU(cudaMemsetAsync(d_tri, 0, n * 4, s));
 		CU(cudaMemcpyAsync(d_u, uniforms, nu * 4, cudaMemcpyHostToDevice, s));
-		CU(launch_event_kat(dg.view, dm.mats.as<DevMaterial>(), kind, n, d_si, d_mi, d_tri, d_u, n_uniforms, d_so, d_mo,
+		CU(launch_event_kat(dg.view, dm.mats.as<DevMaterial>(), phys, kind, n, d_si, d_mi, d_tri, d_u, n_uniforms, d_so, d_mo,
 			d_st, d_se, d_hs, d_us, s));
 		CU(cudaMemcpyAsync(state_out, d_so, n * 28, cudaMemcpyDeviceToHost, s));
 		CU(cudaMemcpyAsync(mat_out, d_mo, n * 4, cudaMemcpyDeviceToHost, s));

@@ -107,6 +107,7 @@ void nbl_batch_params_defaults(nbl_batch_params* p)
 	if (!p) return;
 	std::memset(p, 0, sizeof(*p));
 	p->use_graph = 1;
+	nbl_physics_defaults(&p->physics);
 }
 
 nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geometries, nbl_material* const* materials,
@@ -155,7 +156,8 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 			require(materials[i] != nullptr, "null material");
 			ms.push_back(&materials[i]->m);
 		}
-		b->mats.upload(ms, b->stream);
+		const uint32_t phys = physics_bits(params->physics);
+		b->mats.upload(ms, b->stream, phys);
 
 		StepParams& sp = b->sp;
 		sp.mats = b->mats.mats.as<DevMaterial>();
@@ -165,6 +167,7 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 		sp.qcap = factor * cap;
 		sp.ramp = std::max<uint32_t>(cap / 16, 256);
 		sp.refill_below = std::max<uint32_t>(1u, (uint32_t)((double)thr * cap));
+		sp.phys = phys;
 		for (int k = 0; k < 2; ++k)
 			for (int q = 0; q < N_QUEUES; ++q) {
 				DevBuf* qb = b->queues[k][q];

@@ -103,8 +103,9 @@ struct DeviceMaterials {
 	DevBuf tables, mats;
 	int n = 0;
 	std::vector<DevMaterial> host;   // the device array's contents
-	void upload(const std::vector<const HostMaterial*>& ms, cudaStream_t s)
+	void upload(const std::vector<const HostMaterial*>& ms, cudaStream_t s, uint32_t phys = PH_DEFAULT)
 	{
+		const bool kieft = (phys & PH_KIEFT) != 0;
 		n = (int)ms.size();
 		std::vector<float> blob;
 		std::vector<size_t> offs;
@@ -116,7 +117,8 @@ struct DeviceMaterials {
 			blob.insert(blob.end(), t.data.begin(), t.data.end());
 		};
 		for (const HostMaterial* m : ms) {
-			add(m->el_imfp); add(m->el_icdf); add(m->in_imfp); add(m->in_omega); add(m->in_q); add(m->in_binding);
+			const InelasticTables it = inelastic_tables(*m, kieft);
+			add(m->el_imfp); add(m->el_icdf); add(*it.imfp); add(*it.omega); add(*it.q); add(*it.binding);
 		}
 		tables.alloc(std::max<size_t>(blob.size(), 1) * sizeof(float));
 		CU(cudaMemcpyAsync(tables.p, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice, s));
@@ -134,8 +136,9 @@ struct DeviceMaterials {
 		for (size_t i = 0; i < ms.size(); ++i) {
 			const HostMaterial& m = *ms[i];
 			DevMaterial& d = dm[i];
-			d.el_imfp = dev(m.el_imfp); d.el_icdf = dev(m.el_icdf); d.in_imfp = dev(m.in_imfp);
-			d.in_omega = dev(m.in_omega); d.in_q = dev(m.in_q); d.in_binding = dev(m.in_binding);
+			const InelasticTables it = inelastic_tables(m, kieft);
+			d.el_imfp = dev(m.el_imfp); d.el_icdf = dev(m.el_icdf); d.in_imfp = dev(*it.imfp);
+			d.in_omega = dev(*it.omega); d.in_q = dev(*it.q); d.in_binding = dev(*it.binding);
 			d.fermi = m.fermi; d.band_gap = m.band_gap; d.barrier = m.barrier;
 			d.phonon_loss = m.phonon_loss; d.recoil_const = m.recoil_const;
 			d.in_scale = 1.0f; d.el_scale = 1.0f; d.pad = 0;

@@ -57,10 +57,32 @@ struct HostTable {
 };
 
 // Material (core/material.h:19-46): the scatter-model tables and constants.
+// Full-Penn tables (in_*) and Kieft-Bosch inelastic tables (ki_*) are each
+// present when `models` has bit 0 / bit 1 set.
 struct HostMaterial {
 	HostTable el_imfp, el_icdf, in_imfp, in_omega, in_q, in_binding;
 	float fermi = 0, band_gap = -1, barrier = 0, phonon_loss = 0, recoil_const = 0;
+	int32_t models = 0;
+	HostTable ki_imfp, ki_w0, ki_binding;
 };
+
+// The inelastic tables a run of the selected model reads, in the order of
+// DevMaterial's in_imfp, in_omega, in_q, in_binding (the Kieft-Bosch model
+// reads no q table: a one-point placeholder stands in).
+struct InelasticTables { const HostTable *imfp, *omega, *q, *binding; };
+inline InelasticTables inelastic_tables(const HostMaterial& m, bool kieft)
+{
+	static const HostTable unused = [] { HostTable t; t.data.assign(1, 0.0f); return t; }();
+	if (kieft) {
+		require(m.models & 2, "material has no Kieft-Bosch inelastic tables");
+		return { &m.ki_imfp, &m.ki_w0, &unused, &m.ki_binding };
+	}
+	require(m.models & 1, "material has no Full-Penn inelastic tables");
+	return { &m.in_imfp, &m.in_omega, &m.in_q, &m.in_binding };
+}
+
+// nbl_physics_opts -> PH_* bits; every option must be 0 or 1.
+uint32_t physics_bits(const nbl_physics_opts& o);
 
 HostMaterial load_material_file(const std::string& path);
 

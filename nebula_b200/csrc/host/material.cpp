@@ -5,7 +5,8 @@
 // (io/hdf5_file.h:27-177): quantity properties with units, float datasets
 // with a unit and a dimension scale per axis.  The transforms applied on
 // load are those of kieft_elastic::create (physics/kieft/elastic.h:120-166),
-// full_penn::create (physics/full_penn.h:294-406) and material(hdf5_file)
+// full_penn::create (physics/full_penn.h:294-406), kieft_inelastic::create
+// (physics/kieft/inelastic.h:215-331) and material(hdf5_file)
 // (core/material.inl:13-18); the double/float evaluation order follows them
 // (and units::quantity, common/units/quantity.h, where eV, nm and
 // dimensionless are 1 and g is 6.2415e15), so the tables equal the
@@ -26,6 +27,15 @@ struct File {
 	std::map<std::string, std::pair<double, std::string>> props;
 	std::map<std::string, Dataset> sets;
 };
+
+// HDF5 resolves "a/b" and "/a/b" to the same dataset (the reference asks
+// for "ionization/binding_icdf" in kieft/inelastic.h:263).
+std::string canonical(const std::string& name)
+{
+	size_t i = 0;
+	while (i < name.size() && name[i] == '/') ++i;
+	return name.substr(i);
+}
 
 File parse(const std::string& path)
 {
@@ -78,7 +88,7 @@ File parse(const std::string& path)
 		need(4 * cnt);
 		std::memcpy(d.data.data(), &b[off], 4 * cnt);
 		off += 4 * cnt;
-		out.sets[k] = std::move(d);
+		out.sets[canonical(k)] = std::move(d);
 	}
 	return out;
 }
@@ -126,6 +136,73 @@ void axis(int32_t n, double lo, double hi, bool log_axis, float& vmin, float& vs
 	vstep = (n - 1) / (b - a);
 }
 
+// table_2D::get_rounddown (table_2D.inl:96-104) on the host
+float rounddown2(const HostTable& t, float x, float y)
+{
+	const float xi = (x - t.x_min) * t.x_step;
+	const float yi = (y - t.y_min) * t.y_step;
+	const int ix = std::min(std::max((int)std::floor(xi), 0), t.nx - 1);
+	const int iy = std::min(std::max((int)std::floor(yi), 0), t.ny - 1);
+	return t.data[(size_t)ix * t.ny + iy];
+}
+
+// Ionisation table of the Kieft-Bosch model (kieft/inelastic.h:262-327):
+// above 100 eV an inner shell from the binding ICDF at K + 10 eV (kept when
+// >= 50 eV and finite), otherwise the largest outer shell (< 100 eV) not
+// above K, otherwise -1.  The reference rewrites the table in place, row by
+// row, while it reads it with get_rounddown, so later reads may see values
+// already rewritten; the same order is kept here.
+void load_kieft_binding(const std::string& path, Dataset& d, Dataset& shells, HostTable& t)
+{
+	double lo, hi;
+	t.data = d.data;
+	t.nx = (int32_t)d.dims[0]; t.ny = (int32_t)d.dims[1];
+	log_range(d.scales[0], lo, hi); axis(t.nx, lo, hi, true, t.x_min, t.x_step);
+	lin_range(d.scales[1], t.ny, lo, hi); axis(t.ny, lo, hi, false, t.y_min, t.y_step);
+	std::vector<double> outer;
+	{
+		const double u = unit_value(shells.unit);
+		for (float v : shells.data) {
+			const double e = (double)v * u;
+			if (e < 100)
+				outer.push_back(e);
+		}
+		std::sort(outer.begin(), outer.end());
+	}
+	const double unit = unit_value(d.unit);
+	const Scale& ks = d.scales[0];
+	require(ks.present, path + ": binding_icdf energy scale missing", NBL_ERR_IO);
+	const double ku = unit_value(ks.unit);
+	const double kfirst = ks.v.front() * ku;
+	const double kstep = std::log((ks.v.back() * ku) / kfirst) / (ks.v.size() - 1);
+	double pfirst = 0, plast = 1;
+	if (d.scales[1].present) {
+		const double pu = unit_value(d.scales[1].unit);
+		pfirst = d.scales[1].v.front() * pu;
+		plast = d.scales[1].v.back() * pu;
+	}
+	const double pstep = (plast - pfirst) / (t.ny - 1);
+	for (int32_t x = 0; x < t.nx; ++x) {
+		const double K = kfirst * std::exp(x * kstep);
+		for (int32_t y = 0; y < t.ny; ++y) {
+			const float P = (float)(pfirst + y * pstep);
+			const double margin = 10;
+			double binding = -1;
+			if (K > 100) {
+				binding = (double)rounddown2(t, (float)std::log((K + margin) / 1.0), P) * unit;
+				if (binding < 50 || !std::isfinite(binding))
+					binding = -1;
+			}
+			if (binding < 0) {
+				// largest outer shell <= K
+				for (auto it = outer.rbegin(); it != outer.rend(); ++it)
+					if (!(*it > K)) { binding = *it; break; }
+			}
+			t.data[(size_t)x * t.ny + y] = (float)(binding / 1.0);
+		}
+	}
+}
+
 }  // namespace
 
 HostMaterial load_material_file(const std::string& path)
@@ -136,8 +213,9 @@ HostMaterial load_material_file(const std::string& path)
 		require(it != f.props.end(), path + ": missing property '" + k + "'", NBL_ERR_IO);
 		return it->second.first * unit_value(it->second.second);
 	};
+	auto has = [&](const char* k) { return f.sets.count(canonical(k)) != 0; };
 	auto set = [&](const char* k, size_t rank) -> Dataset& {
-		auto it = f.sets.find(k);
+		auto it = f.sets.find(canonical(k));
 		require(it != f.sets.end(), path + ": missing table '" + k + "'", NBL_ERR_IO);
 		require(it->second.dims.size() == rank, path + ": table '" + k + "' has the wrong rank", NBL_ERR_IO);
 		return it->second;
@@ -145,12 +223,14 @@ HostMaterial load_material_file(const std::string& path)
 	HostMaterial m;
 	double lo, hi;
 
-	// inverse mean free paths: log(imfp * unit) (elastic.h:129-140, full_penn.h:306-317)
-	const char* imfp_names[2] = { "/elastic/imfp", "/full_penn/imfp" };
-	HostTable* imfp_tabs[2] = { &m.el_imfp, &m.in_imfp };
-	for (int k = 0; k < 2; ++k) {
-		Dataset& d = set(imfp_names[k], 1);
-		HostTable& t = *imfp_tabs[k];
+	const bool penn = has("/full_penn/imfp"), kieft = has("/inelastic_kieft/imfp");
+	require(penn || kieft, path + ": no inelastic model tables (/full_penn or /inelastic_kieft)", NBL_ERR_IO);
+	m.models = (penn ? 1 : 0) | (kieft ? 2 : 0);
+
+	// inverse mean free paths: log(imfp * unit) (elastic.h:129-140,
+	// full_penn.h:306-317, kieft/inelastic.h:226-238)
+	auto imfp = [&](const char* name, HostTable& t) {
+		Dataset& d = set(name, 1);
 		t.data = d.data;
 		const float unit = (float)(unit_value(d.unit) * 1.0);
 		for (float& v : t.data)
@@ -158,7 +238,8 @@ HostMaterial load_material_file(const std::string& path)
 		t.nx = (int32_t)d.dims[0];
 		log_range(d.scales[0], lo, hi);
 		axis(t.nx, lo, hi, true, t.x_min, t.x_step);
-	}
+	};
+	imfp("/elastic/imfp", m.el_imfp);
 	{	// cos(theta) ICDF clipped to [-1, 1] (elastic.h:144-157)
 		Dataset& d = set("/elastic/costheta_icdf", 2);
 		HostTable& t = m.el_icdf;
@@ -170,9 +251,10 @@ HostMaterial load_material_file(const std::string& path)
 		lin_range(d.scales[1], t.ny, lo, hi); axis(t.ny, lo, hi, false, t.y_min, t.y_step);
 	}
 	const double fermi_q = prop("fermi");
-	{	// omega ICDF: log(max(0, min(K - fermi, omega))) (full_penn.h:321-344)
-		Dataset& d = set("/full_penn/omega_icdf", 2);
-		HostTable& t = m.in_omega;
+	// energy-loss ICDF: log(max(0, min(K - fermi, omega))) (full_penn.h:321-344,
+	// kieft/inelastic.h:240-261)
+	auto loss_icdf = [&](const char* name, HostTable& t) {
+		Dataset& d = set(name, 2);
 		t.data = d.data;
 		const float unit = (float)(unit_value(d.unit) / 1.0);
 		const Scale& ks = d.scales[0];
@@ -190,7 +272,10 @@ HostMaterial load_material_file(const std::string& path)
 		t.nx = (int32_t)d.dims[0]; t.ny = (int32_t)d.dims[1];
 		log_range(d.scales[0], lo, hi); axis(t.nx, lo, hi, true, t.x_min, t.x_step);
 		lin_range(d.scales[1], t.ny, lo, hi); axis(t.ny, lo, hi, false, t.y_min, t.y_step);
-	}
+	};
+	if (penn) {
+	imfp("/full_penn/imfp", m.in_imfp);
+	loss_icdf("/full_penn/omega_icdf", m.in_omega);
 	{	// q ICDF in eV^1/2: q * hbar/sqrt(2m) (full_penn.h:348-369)
 		Dataset& d = set("/full_penn/q_icdf", 3);
 		HostTable& t = m.in_q;
@@ -218,6 +303,12 @@ HostMaterial load_material_file(const std::string& path)
 		log_range(d.scales[0], lo, hi); axis(t.nx, lo, hi, true, t.x_min, t.x_step);
 		log_range(d.scales[1], lo, hi); axis(t.ny, lo, hi, true, t.y_min, t.y_step);
 		lin_range(d.scales[2], t.nz, lo, hi); axis(t.nz, lo, hi, false, t.z_min, t.z_step);
+	}
+	}
+	if (kieft) {
+		imfp("/inelastic_kieft/imfp", m.ki_imfp);
+		loss_icdf("/inelastic_kieft/w0_icdf", m.ki_w0);
+		load_kieft_binding(path, set("ionization/binding_icdf", 2), set("ionization/outer_shells", 1), m.ki_binding);
 	}
 	m.fermi = (float)(fermi_q / 1.0);
 	{

@@ -70,6 +70,7 @@ struct StepParams {
 	uint32_t max_events;      // per-electron event budget
 	int32_t adjoint;          // accumulate score functions
 	uint32_t refill_below;    // refill primaries only while fewer electrons are in flight
+	uint32_t phys;            // physics selection (PH_* bits)
 };
 
 // One job of a batched run: its geometry, its primaries (a contiguous range
@@ -102,7 +103,7 @@ cudaError_t launch_ray_query(const DevGeometry& g, const float* pos, const float
 	cudaStream_t s);
 cudaError_t launch_table_kat(const DevMaterial* mat, int which, int rounddown, int64_t n,
 	const float* x, const float* y, const float* z, float* out, cudaStream_t s);
-cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, int kind, int64_t n,
+cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, uint32_t phys, int kind, int64_t n,
 	const float* state_in, const int32_t* mat_in, const int32_t* tri, const float* uniforms, int32_t n_uniforms,
 	float* state_out, int32_t* mat_out, int32_t* status, float* se_out, int32_t* has_se, int32_t* used,
 	cudaStream_t s);

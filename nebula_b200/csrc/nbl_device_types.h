@@ -51,6 +51,25 @@ struct DevTable {
 	float x_min, x_step, y_min, y_step, z_min, z_step;
 };
 
+// Physics selection (physics_config.h:20-46 and the option bools of the
+// models it names), one bit per option, read by every event.
+enum : uint32_t {
+	PH_GEN_SE = 1u << 0,        // full_penn / kieft_inelastic generate_secondary
+	PH_PHONON = 1u << 1,        // kieft_elastic acoustic_phonon_loss
+	PH_RECOIL = 1u << 2,        // kieft_elastic atomic_recoil_loss
+	PH_QT = 1u << 3,            // boundary_intersect quantum_transmission
+	PH_REFRACT = 1u << 4,       // boundary_intersect interface_refraction
+	PH_ABSORB = 1u << 5,        // boundary_intersect interface_absorption
+	PH_OPT_PHONON = 1u << 6,    // kieft_inelastic optical_phonon_loss
+	PH_INST_MOM = 1u << 7,      // kieft_inelastic instantaneous_momentum
+	PH_MOM_CONS = 1u << 8,      // kieft_inelastic momentum_conservation
+	PH_KIEFT = 1u << 16,        // inelastic model: kieft_inelastic instead of full_penn
+	PH_DEFAULT = PH_GEN_SE | PH_PHONON | PH_RECOIL | PH_QT | PH_REFRACT | PH_OPT_PHONON | PH_INST_MOM | PH_MOM_CONS,
+};
+
+// Inelastic tables by model: Full Penn uses in_imfp, in_omega (log omega
+// ICDF), in_q and in_binding (3-D); Kieft-Bosch uses in_imfp, in_omega (log
+// omega' ICDF) and in_binding (2-D), in_q unused.
 struct DevMaterial {
 	DevTable el_imfp, el_icdf, in_imfp, in_omega, in_q, in_binding;
 	float fermi, band_gap, barrier, phonon_loss, recoil_const;

@@ -110,10 +110,8 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		require(n_materials >= 1 && n_materials <= NBL_NOALLOC_MAX_MATERIALS,
 			"nbl_run_noalloc: at most " + std::to_string(NBL_NOALLOC_MAX_MATERIALS) + " materials");
 		require(params->adjoint == 0, "nbl_run_noalloc: the adjoint is not available without allocation");
-		const nbl_physics_opts& ph = params->physics;
-		require(ph.inelastic_model == 0 && ph.generate_secondaries == 1 && ph.acoustic_phonon_loss == 1 &&
-			ph.atomic_recoil_loss == 1 && ph.quantum_transmission == 1 && ph.interface_refraction == 1 &&
-			ph.interface_absorption == 0, "only the reference's default physics selection is built");
+		const uint32_t phys = physics_bits(params->physics);
+		const bool kieft = (phys & PH_KIEFT) != 0;
 		const uint32_t cap = params->capacity ? params->capacity : NA_CAPACITY;
 		require(cap >= 32 && cap <= NA_CAPACITY, "nbl_run_noalloc: capacity must be 32.." + std::to_string(NA_CAPACITY));
 		int max_mat = -1;
@@ -128,7 +126,8 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		for (int i = 0; i < n_materials; ++i) {
 			require(materials[i] != nullptr, "null material");
 			const HostMaterial& m = materials[i]->m;
-			for (const HostTable* t : { &m.el_imfp, &m.el_icdf, &m.in_imfp, &m.in_omega, &m.in_q, &m.in_binding })
+			const InelasticTables it = inelastic_tables(m, kieft);
+			for (const HostTable* t : { &m.el_imfp, &m.el_icdf, it.imfp, it.omega, it.q, it.binding })
 				table_bytes += align_up(t->data.size() * sizeof(float));
 		}
 		require(table_bytes <= NA_TABLE_BYTES,
@@ -186,8 +185,9 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 				return d;
 			};
 			DevMaterial& d = dm[i];
-			d.el_imfp = put(m.el_imfp); d.el_icdf = put(m.el_icdf); d.in_imfp = put(m.in_imfp);
-			d.in_omega = put(m.in_omega); d.in_q = put(m.in_q); d.in_binding = put(m.in_binding);
+			const InelasticTables it = inelastic_tables(m, kieft);
+			d.el_imfp = put(m.el_imfp); d.el_icdf = put(m.el_icdf); d.in_imfp = put(*it.imfp);
+			d.in_omega = put(*it.omega); d.in_q = put(*it.q); d.in_binding = put(*it.binding);
 			d.fermi = m.fermi; d.band_gap = m.band_gap; d.barrier = m.barrier;
 			d.phonon_loss = m.phonon_loss; d.recoil_const = m.recoil_const;
 			d.in_scale = 1.0f; d.el_scale = 1.0f; d.pad = 0;
@@ -226,6 +226,7 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		sp.capacity = cap;
 		sp.ramp = std::max<uint32_t>(cap / 16, 256);
 		sp.refill_below = cap;
+		sp.phys = phys;
 		sp.spill = carve_queue(base + OFF_SPILL, NA_RING);
 		sp.spill_mask = NA_RING - 1;
 		sp.ctrl = reinterpret_cast<uint32_t*>(base + OFF_CTRL);

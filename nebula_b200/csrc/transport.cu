@@ -103,7 +103,10 @@ __global__ void k_table_kat(const DevMaterial* __restrict__ mat, int which, int 
 	case 1: v = rounddown ? table2_rounddown(m.el_icdf, x[i], y[i]) : table2_get(m.el_icdf, x[i], y[i]); break;
 	case 3: v = rounddown ? table2_rounddown(m.in_omega, x[i], y[i]) : table2_get(m.in_omega, x[i], y[i]); break;
 	case 4: v = rounddown ? table3_rounddown(m.in_q, x[i], y[i], z[i]) : table3_get(m.in_q, x[i], y[i], z[i]); break;
-	default: v = rounddown ? table3_rounddown(m.in_binding, x[i], y[i], z[i]) : table3_get(m.in_binding, x[i], y[i], z[i]); break;
+	case 5: v = rounddown ? table3_rounddown(m.in_binding, x[i], y[i], z[i]) : table3_get(m.in_binding, x[i], y[i], z[i]); break;
+	case 6: v = table1_get(m.in_imfp, x[i]); break;
+	case 7: v = rounddown ? table2_rounddown(m.in_omega, x[i], y[i]) : table2_get(m.in_omega, x[i], y[i]); break;
+	default: v = rounddown ? table2_rounddown(m.in_binding, x[i], y[i]) : table2_get(m.in_binding, x[i], y[i]); break;
 	}
 	out[i] = v;
 }
@@ -118,7 +121,7 @@ cudaError_t launch_table_kat(const DevMaterial* mat, int which, int rounddown, i
 }
 
 /* ---------------------------------------------------------- single events */
-__global__ void k_event_kat(const DevGeometry g, const DevMaterial* __restrict__ mats, int kind, int64_t n,
+__global__ void k_event_kat(const DevGeometry g, const DevMaterial* __restrict__ mats, uint32_t ph, int kind, int64_t n,
 	const float* __restrict__ state_in, const int32_t* __restrict__ mat_in, const int32_t* __restrict__ tri,
 	const float* __restrict__ uniforms, int32_t n_uniforms, float* __restrict__ state_out,
 	int32_t* __restrict__ mat_out, int32_t* __restrict__ status, float* __restrict__ se_out,
@@ -140,11 +143,11 @@ __global__ void k_event_kat(const DevGeometry g, const DevMaterial* __restrict__
 	se.pos = v3(0, 0, 0); se.dir = v3(0, 0, 0); se.E = 0;
 	if (kind == 3) {
 		const DevTriangle T = load_tri(g.tris, tri[i]);
-		st = boundary_event(T, mats, p, mat, rng);
+		st = boundary_event(T, mats, p, mat, rng, nullptr, ph);
 	} else if (kind == 1) {
-		spawned = inelastic_event(mats[mat], p, se, rng);
+		spawned = inelastic_event(mats[mat], p, se, rng, ph);
 	} else {
-		elastic_event(mats[mat], p, rng);
+		elastic_event(mats[mat], p, rng, ph);
 	}
 	float* o = state_out + 7 * i;
 	o[0] = p.pos.x; o[1] = p.pos.y; o[2] = p.pos.z; o[3] = p.dir.x; o[4] = p.dir.y; o[5] = p.dir.z; o[6] = p.E;
@@ -156,14 +159,14 @@ __global__ void k_event_kat(const DevGeometry g, const DevMaterial* __restrict__
 	used[i] = (int32_t)rng.n;
 }
 
-cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, int kind, int64_t n,
+cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, uint32_t phys, int kind, int64_t n,
 	const float* state_in, const int32_t* mat_in, const int32_t* tri, const float* uniforms, int32_t n_uniforms,
 	float* state_out, int32_t* mat_out, int32_t* status, float* se_out, int32_t* has_se, int32_t* used,
 	cudaStream_t s)
 {
 	if (n <= 0)
 		return cudaSuccess;
-	k_event_kat<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(g, mats, kind, n, state_in, mat_in, tri, uniforms,
+	k_event_kat<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(g, mats, phys, kind, n, state_in, mat_in, tri, uniforms,
 		n_uniforms, state_out, mat_out, status, se_out, has_se, used);
 	return cudaGetLastError();
 }
@@ -408,26 +411,26 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			const DevTriangle T = load_tri(rv.geom->tris, last_tri);
 			if (ADJ) {
 				BoundaryScore bs = { 0.0f, 0.0f, -1, -1 };
-				status = boundary_event(T, P.mats, p, mat, r, &bs);
+				status = boundary_event(T, P.mats, p, mat, r, &bs, P.phys);
 				// the work function enters through barrier = fermi + W of the
 				// materials on either side of the crossing
 				if (bs.mat_in >= 0 && bs.mat_in < 2) sc[3 * bs.mat_in + 2] += bs.d_in;
 				if (bs.mat_out >= 0 && bs.mat_out < 2) sc[3 * bs.mat_out + 2] += bs.d_out;
 			} else {
-				status = boundary_event(T, P.mats, p, mat, r);
+				status = boundary_event(T, P.mats, p, mat, r, nullptr, P.phys);
 			}
 		} else if (kind == EV_ELASTIC) {
 			lc.add(CNT_ELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
 			r.init(rv.key, event, 1u, stream_tag, lineage);
-			elastic_event(P.mats[mat], p, r);
+			elastic_event(P.mats[mat], p, r, P.phys);
 		} else if (kind == EV_INELASTIC) {
 			lc.add(CNT_INELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
 			r.init(rv.key, event, 1u, stream_tag, lineage);
-			spawn = inelastic_event(P.mats[mat], p, se, r);
+			spawn = inelastic_event(P.mats[mat], p, se, r, P.phys);
 		}
 
 		// detection output: record + tallies

@@ -35,6 +35,26 @@ The physics used to fill the tables (all in float64):
 * no inner shells: the binding table is all zeros, which ``full_penn::create``
   maps to -1 (Fermi-sea excitation only).
 
+``build_raw_material(spec, inelastic="kieft")`` writes the tables of the
+Kieft-Bosch inelastic model instead of Full Penn's
+(``kieft_inelastic::create`` ``physics/kieft/inelastic.h:215-331``):
+
+========================== ========================== ======== ==================
+/inelastic_kieft/imfp      K (log, eV)                nm^-1    inelastic.h:226-238
+/inelastic_kieft/w0_icdf   K (log, eV) x P (lin)      eV       inelastic.h:240-261
+/ionization/binding_icdf   K (log, eV) x P (lin)      eV       inelastic.h:262-327
+/ionization/outer_shells   shell index                eV       inelastic.h:270-282
+========================== ========================== ======== ==================
+
+* the inverse mean free path is the same Drude-Lindhard one;
+* the zero-momentum loss w' follows the optical-data model (Ashley 1988):
+  d(1/lambda)/dw' = 1/(pi a0 K) Im[-1/eps(0, w')] L(w'/K), with
+  L(x) = (1-x) ln(4/x) - 7x/4 + x^(3/2) - 33x^2/32 clipped at 0;
+* inner shells (binding >= 50 eV) take a Bethe-like share of the events,
+  f(K) = c ln(K/B) / (K/B) above B, placed at the top of the probability
+  axis; the rest of the axis is 0 (no inner shell);
+* outer shells: the valence binding energies of the material's elements.
+
 Everything here is seeded-free and deterministic: the same call gives the
 same bytes.
 """
@@ -81,6 +101,14 @@ def silicon(e_max: float = 10e3) -> MaterialSpec:
     return MaterialSpec("silicon", Z=14.0, atom_density=49.94, plasmon=16.6,
                         damping=4.0, fermi=7.8, work_function=4.8, band_gap=1.1,
                         phonon_loss=0.05, effective_A=28.0855, e_max=e_max)
+
+
+# Kieft-Bosch model: (binding eV, share scale c) of the inner shells and the
+# valence (outer-shell) binding energies, per material name (Si: 2p, 2s, 1s;
+# 3p, 3s.  PMMA: C 1s, O 1s; C 2p, O 2p, C 2s).
+INNER_SHELLS = {"silicon": [(99.42, 0.06), (149.7, 0.02), (1839.0, 0.01)],
+                "pmma": [(284.2, 0.05), (543.1, 0.02)]}
+OUTER_SHELLS = {"silicon": [8.15, 13.46], "pmma": [11.26, 13.62, 16.59]}
 
 
 def pmma(e_max: float = 10e3) -> MaterialSpec:
@@ -193,8 +221,55 @@ def q_icdf_table(spec: MaterialSpec, energies, wk, probs, n_q=256):
     return out
 
 
+def ashley_L(x):
+    x = np.asarray(x, dtype=np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        v = (1 - x) * np.log(4 / x) - 1.75 * x + x ** 1.5 - 33.0 / 32.0 * x * x
+    return np.where(np.isfinite(v) & (v > 0), v, 0.0)
+
+
+def kieft_w0_icdf(spec: MaterialSpec, energies, probs, n_w=1024):
+    """ICDF of the zero-momentum loss w' (eV) over (K, P), optical-data model."""
+    out = np.empty((len(energies), len(probs)))
+    for i, K in enumerate(energies):
+        w_hi = K - spec.fermi
+        if w_hi <= 2e-3:
+            out[i, :] = max(w_hi, 1e-3)
+            continue
+        w = np.exp(np.linspace(np.log(1e-3), np.log(w_hi), n_w))
+        dens = drude_lindhard_elf(0.0, w, spec) * ashley_L(w / K)
+        cdf = np.concatenate([[0.0], np.cumsum(0.5 * (dens[1:] + dens[:-1]) * np.diff(w))])
+        if not np.isfinite(cdf[-1]) or cdf[-1] <= 0:
+            out[i, :] = w[0]
+            continue
+        cdf = cdf / cdf[-1]
+        cdf = np.maximum.accumulate(cdf + np.arange(len(cdf)) * 1e-15)
+        cdf /= cdf[-1]
+        out[i, :] = np.interp(probs, cdf, w)
+    return out
+
+
+def kieft_binding_icdf(spec: MaterialSpec, energies, probs):
+    """Binding energy (eV) over (K, P): inner shells at the top of the P axis
+    with Bethe-like shares, 0 (no inner shell) elsewhere."""
+    out = np.zeros((len(energies), len(probs)))
+    for i, K in enumerate(energies):
+        top = 1.0
+        for B, c in INNER_SHELLS.get(spec.name, []):
+            if K <= B:
+                continue
+            u = K / B
+            share = c * np.log(u) / u * np.e          # peaks at c for K = e B
+            lo = top - share
+            out[i, (probs >= lo) & (probs < top)] = B
+            if top >= 1.0:
+                out[i, probs >= 1.0] = B
+            top = lo
+    return out
+
+
 # ----------------------------------------------------------------------------
-def build_raw_material(spec: MaterialSpec) -> dict:
+def build_raw_material(spec: MaterialSpec, inelastic: str = "full_penn") -> dict:
     """Raw material content (datasets with dimension scales, properties).
 
     The result has the structure of a Nebula material file: it is what
@@ -207,6 +282,29 @@ def build_raw_material(spec: MaterialSpec) -> dict:
 
     el_imfp = elastic_imfp(K, spec)
     el_icdf = elastic_costheta_icdf(K, P, spec)
+    props = {
+        "fermi": (spec.fermi, "eV"),
+        "barrier": (spec.barrier, "eV"),
+        "band_gap": (spec.band_gap, "eV"),
+        "phonon_loss": (spec.phonon_loss, "eV"),
+        "effective_A": (spec.effective_A * AMU_G, "g"),
+        "work_function": (spec.work_function, "eV"),
+    }
+    if inelastic == "kieft":
+        in_imfp, _ = inelastic_tables(spec, K, P)
+        datasets = {
+            "/elastic/imfp": dict(unit="nm^-1", data=el_imfp, scales=[("eV", K)]),
+            "/elastic/costheta_icdf": dict(unit="", data=el_icdf, scales=[("eV", K), ("", P)]),
+            "/inelastic_kieft/imfp": dict(unit="nm^-1", data=in_imfp, scales=[("eV", K)]),
+            "/inelastic_kieft/w0_icdf": dict(unit="eV", data=kieft_w0_icdf(spec, K, P), scales=[("eV", K), ("", P)]),
+            "/ionization/binding_icdf": dict(unit="eV", data=kieft_binding_icdf(spec, K, P),
+                                             scales=[("eV", K), ("", P)]),
+            "/ionization/outer_shells": dict(unit="eV", data=np.asarray(OUTER_SHELLS[spec.name], np.float64),
+                                             scales=[None]),
+        }
+        return dict(name=spec.name, datasets=datasets, properties=props)
+    if inelastic != "full_penn":
+        raise ValueError("inelastic model must be 'full_penn' or 'kieft'")
     in_imfp, omega = inelastic_tables(spec, K, P)
     q = q_icdf_table(spec, K, WK, P)
 
@@ -223,13 +321,5 @@ def build_raw_material(spec: MaterialSpec) -> dict:
                                   scales=[("eV", K), ("", WK), ("", P)]),
         "/ionization/binding_icdf": dict(unit="eV", data=np.zeros((2, 2, 2)),
                                          scales=[("eV", Kb), ("", Wb), ("", Pb)]),
-    }
-    props = {
-        "fermi": (spec.fermi, "eV"),
-        "barrier": (spec.barrier, "eV"),
-        "band_gap": (spec.band_gap, "eV"),
-        "phonon_loss": (spec.phonon_loss, "eV"),
-        "effective_A": (spec.effective_A * AMU_G, "g"),
-        "work_function": (spec.work_function, "eV"),
     }
     return dict(name=spec.name, datasets=datasets, properties=props)

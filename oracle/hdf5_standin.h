@@ -107,14 +107,25 @@ public:
 			need(4 * count);
 			std::memcpy(d.data.data(), buf.data() + off, 4 * count);
 			off += 4 * count;
-			_sets[name] = d;
+			_sets[canonical(name)] = d;
 		}
+	}
+
+	// HDF5 resolves "a/b" and "/a/b" alike (the reference asks for both
+	// forms, e.g. kieft/inelastic.h:263 and full_penn.h:374)
+	static std::string canonical(std::string const & name)
+	{
+		size_t i = 0;
+		while (i < name.size() && name[i] == '/')
+			++i;
+		return name.substr(i);
 	}
 
 	std::string const & get_filename() const { return _filename; }
 
-	bool exists(std::string const & name) const
+	bool exists(std::string const & query) const
 	{
+		const std::string name = canonical(query);
 		if (_sets.count(name))
 			return true;
 		// group paths ("/elastic") exist when a dataset lives under them
@@ -224,7 +235,7 @@ private:
 
 	dataset const & get(std::string const & name, int ndim) const
 	{
-		auto it = _sets.find(name);
+		auto it = _sets.find(canonical(name));
 		if (it == _sets.end())
 			throw std::runtime_error("Could not read table '" + name + '\'');
 		if (ndim >= 0 && it->second.dims.size() != (size_t)ndim)

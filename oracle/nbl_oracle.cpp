@@ -23,6 +23,7 @@
 #include <atomic>
 #include <limits>
 #include <algorithm>
+#include <functional>
 
 namespace {
 
@@ -364,7 +365,15 @@ struct manager {
 };
 
 /* ------------------------------------------------------------ physics */
-// kieft_elastic::execute (physics/kieft/elastic.h:67-115), both loss options on
+enum : uint32_t {
+	PH_GEN_SE = 1, PH_PHONON = 2, PH_RECOIL = 4, PH_QT = 8, PH_REFRACT = 16, PH_ABSORB = 32,
+	PH_OPT_PHONON = 64, PH_INST_MOM = 128, PH_MOM_CONS = 256, PH_KIEFT = 65536,
+	PH_DEFAULT = 1 | 2 | 4 | 8 | 16 | 64 | 128 | 256
+};
+uint32_t g_phys = PH_DEFAULT;
+
+// kieft_elastic<cpu, acoustic_phonon_loss, atomic_recoil_loss>::execute
+// (physics/kieft/elastic.h:67-115)
 void elastic(const orc_material& m, pstate& ps, orc_rng* rng)
 {
 	pstate p = ps;
@@ -375,15 +384,17 @@ void elastic(const orc_material& m, pstate& ps, orc_rng* rng)
 	p.dir = normalised(p.dir);
 	const v3 normal_dir = normalised(make_normal_vec(p.dir, rphi(rng)));
 	p.dir = add(mul(p.dir, cos_theta), mul(normal_dir, sin_theta));
-	if (p.E < 200)
-		p.E -= minr(50e-3f, m.phonon_loss);
-	else
+	if (p.E < 200) {
+		if (g_phys & PH_PHONON)
+			p.E -= minr(50e-3f, m.phonon_loss);
+	} else if (g_phys & PH_RECOIL) {
 		p.E -= m.recoil_const * (1 - cos_theta) * p.E;
+	}
 	ps = p;
 }
 
-// full_penn::execute (physics/full_penn.h:62-288), secondaries on
-void inelastic(const orc_material& m, manager& mgr, size_t idx, orc_rng* rng)
+// full_penn<cpu, generate_secondary>::execute (physics/full_penn.h:62-288)
+void inelastic_penn(const orc_material& m, manager& mgr, size_t idx, orc_rng* rng)
 {
 	pstate p = mgr.p[idx];
 	float omega;
@@ -422,6 +433,8 @@ void inelastic(const orc_material& m, manager& mgr, size_t idx, orc_rng* rng)
 			p.E -= omega;
 			p.dir = add(mul(p.dir, c2), mul(prim_normal_dir, s2));
 			mgr.p[idx] = p;
+			if (!(g_phys & PH_GEN_SE))
+				return;
 
 			const v3 se_pos = p.pos;
 			v3 se_dir;
@@ -478,13 +491,91 @@ void inelastic(const orc_material& m, manager& mgr, size_t idx, orc_rng* rng)
 	sdir = normalised(sdir);
 	sdir = add(sdir, smul(std::sqrt(binding / dK), uniform_vector(rng)));
 	sdir = normalised(sdir);
-	mgr.create_secondary(idx, p.pos, sdir, m.fermi + omega - binding);
+	if (g_phys & PH_GEN_SE)
+		mgr.create_secondary(idx, p.pos, sdir, m.fermi + omega - binding);
 	p.E -= omega;
 	p.dir = sub(p.dir, smul(cos_theta, sdir));
 	mgr.p[idx] = p;
 }
 
-// boundary_intersect<true,true,false>::execute (physics/boundary_intersect.h:38-155)
+// kieft_inelastic<cpu, optical_phonon_loss, generate_secondary,
+// instantaneous_momentum, momentum_conservation>::execute
+// (physics/kieft/inelastic.h:63-209)
+void inelastic_kieft(const orc_material& m, manager& mgr, size_t idx, orc_rng* rng)
+{
+	pstate p = mgr.p[idx];
+	float omega0;
+	{	// zero-momentum loss (thesis T.V. eq. 3.82)
+		const float x = std::log(p.E);
+		const float y = orc_rng_unit(rng);
+		omega0 = std::exp(t2_get(m.ki_w0, x, y));
+	}
+	float binding;
+	{
+		const float x = std::log(omega0);
+		const float y = orc_rng_unit(rng);
+		binding = t2_rd(m.ki_binding, x, y);
+	}
+	float omega;
+	{	// Ashley's total loss between the kinematic limits (eq. 3.85)
+		const float omega_max = 0.5f * (p.E + omega0 - m.fermi);
+		float omega_min = omega0;
+		float w0 = minr(omega0 - 1, maxr(0, binding) - m.fermi);
+		if (p.E > 2 * omega0) {
+			omega_min = 0.5f * (p.E + omega0 - std::sqrt(p.E * (p.E - 2 * omega0)));
+			w0 = omega0;
+		}
+		const float U = orc_rng_unit(rng);
+		if ((w0 > 0) && (omega_min > w0) && (omega_min < omega_max)) {
+			const float f_min = 1 / w0 * std::log((omega_min - w0) / omega_min);
+			const float f_max = 1 / w0 * std::log((omega_max - w0) / omega_max);
+			omega = -w0 / std::expm1(w0 * (f_min * (1 - U) + f_max * U));
+		} else {
+			omega = omega0 * omega_max / (omega0 * (1 - U) + omega_max * U);
+		}
+	}
+	if (binding < 0) {
+		if (m.band_gap < 0) {
+			// metals: left open by the reference
+		} else if (omega0 > m.band_gap) {
+			binding = m.band_gap;
+		} else {
+			if (g_phys & PH_OPT_PHONON) {
+				p.E -= omega0;
+				mgr.p[idx] = p;
+			}
+			return;
+		}
+	}
+	binding = maxr(0, binding);
+	p.dir = normalised(p.dir);
+	const v3 normal_dir = normalised(make_normal_vec(p.dir, rphi(rng)));
+	const float K = p.E - m.fermi + 2 * binding;
+	const float dK = binding + omega;
+	const float cos_theta = std::sqrt(dK / K);
+	const float sin_theta = std::sqrt(1 - clampr(cos_theta * cos_theta, 0, 1));
+	v3 sdir = add(mul(p.dir, cos_theta), mul(normal_dir, sin_theta));
+	if (g_phys & PH_INST_MOM) {
+		sdir = normalised(sdir);
+		sdir = add(sdir, smul(std::sqrt(binding / dK), uniform_vector(rng)));
+	}
+	sdir = normalised(sdir);
+	if (g_phys & PH_GEN_SE)
+		mgr.create_secondary(idx, p.pos, sdir, m.fermi + omega - binding);
+	p.E -= omega;
+	if (g_phys & PH_MOM_CONS)
+		p.dir = sub(p.dir, smul(cos_theta, sdir));
+	mgr.p[idx] = p;
+}
+
+void inelastic(const orc_material& m, manager& mgr, size_t idx, orc_rng* rng)
+{
+	if (g_phys & PH_KIEFT) inelastic_kieft(m, mgr, idx, rng);
+	else inelastic_penn(m, mgr, idx, rng);
+}
+
+// boundary_intersect<quantum_transmission, interface_refraction,
+// interface_absorption>::execute (physics/boundary_intersect.h:38-155)
 void boundary(const orc_geometry* g, const orc_material* mats, pstate& ps, orc_rng* rng)
 {
 	pstate p = ps;
@@ -508,12 +599,19 @@ void boundary(const orc_geometry* g, const orc_material* mats, pstate& ps, orc_r
 	if (mout >= 0) dU += mats[mout].barrier;
 	if (p.E * c * c + dU > 0) {
 		const float s = std::sqrt(1 + dU / (p.E * c * c));
-		const float Tr = 4 * s / ((1 + s) * (1 + s));
+		const float Tr = (g_phys & PH_QT) ? 4 * s / ((1 + s) * (1 + s)) : 1;
 		if (orc_rng_unit(rng) < Tr) {
-			p.dir = add(sub(nd, mul(n, c)), mul(smul(s, n), c));
+			if (g_phys & PH_REFRACT)
+				p.dir = add(sub(nd, mul(n, c)), mul(smul(s, n), c));
 			p.E += dU;
 			p.material = mout;
 			ps = p;
+			return;
+		}
+	}
+	if (g_phys & PH_ABSORB) {
+		if (dU < 0 && orc_rng_unit(rng) < std::exp(1 + 0.5f * p.E / dU)) {
+			ps.status = TERMINATED;
 			return;
 		}
 	}
@@ -551,7 +649,8 @@ struct driver {
 				if (path < distance) { distance = path; type = 2; }
 			}
 			{
-				const float imfp = std::exp(t1_get(m.in_imfp, std::log(p.E)));
+				const orc_table& it = (g_phys & PH_KIEFT) ? m.ki_imfp : m.in_imfp;
+				const float imfp = std::exp(t1_get(it, std::log(p.E)));
 				const float path = rexponential(rng, 1 / imfp);
 				if (path < distance) { distance = path; type = 1; }
 			}
@@ -627,6 +726,14 @@ struct nm_scale { bool present = false; std::string unit; std::vector<double> v;
 struct nm_set { std::string unit; std::vector<uint64_t> dims; std::vector<nm_scale> scales; std::vector<float> data; };
 struct nm_file { std::map<std::string, std::pair<double, std::string>> props; std::map<std::string, nm_set> sets; };
 
+// HDF5 resolves "a/b" and "/a/b" to the same dataset
+std::string canonical(const std::string& name)
+{
+	size_t i = 0;
+	while (i < name.size() && name[i] == '/') ++i;
+	return name.substr(i);
+}
+
 nm_file read_nmat(const char* path)
 {
 	std::ifstream f(path, std::ios::binary);
@@ -654,7 +761,7 @@ nm_file read_nmat(const char* path)
 		}
 		size_t cnt = 1; for (auto d : s.dims) cnt *= d;
 		s.data.resize(cnt); need(4 * cnt); std::memcpy(s.data.data(), &b[off], 4 * cnt); off += 4 * cnt;
-		out.sets[k] = s;
+		out.sets[canonical(k)] = s;
 	}
 	return out;
 }
@@ -689,8 +796,9 @@ void lin_range(const nm_scale& s, size_t n, double& first, double& last)
 
 struct owned_material {
 	orc_material m;
-	std::vector<float> store[6];
+	std::vector<float> store[9];
 };
+
 
 void set_axis(int32_t n, double lo, double hi, bool log_axis, float& vmin, float& vstep)
 {
@@ -713,17 +821,23 @@ extern "C" void* orc_material_load(const char* path, char* err, int errlen)
 			return it->second.first * unit_value(it->second.second);
 		};
 		auto set = [&](const char* k) -> nm_set& {
-			auto it = f.sets.find(k);
+			auto it = f.sets.find(canonical(k));
 			if (it == f.sets.end()) throw std::runtime_error(std::string("missing dataset ") + k);
 			return it->second;
 		};
+		const bool penn = f.sets.count("full_penn/imfp") != 0, kieft = f.sets.count("inelastic_kieft/imfp") != 0;
+		if (!penn && !kieft) throw std::runtime_error("no inelastic model tables");
+		o->m.models = (penn ? 1 : 0) | (kieft ? 2 : 0);
 		double lo, hi;
-		// elastic imfp (elastic.h:129-140) and inelastic imfp (full_penn.h:306-317)
-		const char* imfp_names[2] = { "/elastic/imfp", "/full_penn/imfp" };
-		orc_table* imfp_tabs[2] = { &o->m.el_imfp, &o->m.in_imfp };
-		for (int k = 0; k < 2; ++k) {
+		// elastic imfp (elastic.h:129-140), inelastic imfp (full_penn.h:306-317,
+		// kieft/inelastic.h:226-238)
+		const char* imfp_names[3] = { "/elastic/imfp", "/full_penn/imfp", "/inelastic_kieft/imfp" };
+		orc_table* imfp_tabs[3] = { &o->m.el_imfp, &o->m.in_imfp, &o->m.ki_imfp };
+		const int imfp_store[3] = { 0, 2, 6 };
+		for (int k = 0; k < 3; ++k) {
+			if ((k == 1 && !penn) || (k == 2 && !kieft)) continue;
 			nm_set& s = set(imfp_names[k]);
-			std::vector<float>& st = o->store[k == 0 ? 0 : 2];
+			std::vector<float>& st = o->store[imfp_store[k]];
 			st = s.data;
 			const float unit = (float)(unit_value(s.unit) * 1.0);
 			for (auto& v : st) v = std::log(v * unit);
@@ -745,9 +859,11 @@ extern "C" void* orc_material_load(const char* path, char* err, int errlen)
 			t.data = st.data();
 		}
 		const double fermi_q = prop("fermi");
-		{	// omega icdf (full_penn.h:321-344)
-			nm_set& s = set("/full_penn/omega_icdf");
-			std::vector<float>& st = o->store[3];
+		// omega icdf (full_penn.h:321-344) / omega' icdf (kieft/inelastic.h:240-261)
+		for (int k = 0; k < 2; ++k) {
+			if ((k == 0 && !penn) || (k == 1 && !kieft)) continue;
+			nm_set& s = set(k == 0 ? "/full_penn/omega_icdf" : "/inelastic_kieft/w0_icdf");
+			std::vector<float>& st = o->store[k == 0 ? 3 : 7];
 			st = s.data;
 			const float unit = (float)(unit_value(s.unit) / 1.0);
 			const nm_scale& ks = s.scales[0];
@@ -761,12 +877,55 @@ extern "C" void* orc_material_load(const char* path, char* err, int errlen)
 					v = (float)std::log(std::max(0.0, std::min<double>((K - fermi_q) / 1.0, v * unit)));
 				}
 			}
-			orc_table& t = o->m.in_omega;
+			orc_table& t = k == 0 ? o->m.in_omega : o->m.ki_w0;
 			t.nx = (int32_t)s.dims[0]; t.ny = (int32_t)s.dims[1]; t.nz = 1;
 			log_range(s.scales[0], lo, hi); set_axis(t.nx, lo, hi, true, t.x_min, t.x_step);
 			lin_range(s.scales[1], t.ny, lo, hi); set_axis(t.ny, lo, hi, false, t.y_min, t.y_step);
 			t.data = st.data();
 		}
+		if (kieft) {	// ionisation table (kieft/inelastic.h:262-327)
+			nm_set& s = set("ionization/binding_icdf");
+			nm_set& sh = set("ionization/outer_shells");
+			if (s.dims.size() != 2) throw std::runtime_error("Kieft binding table must be 2-D");
+			std::vector<float>& st = o->store[8];
+			st = s.data;
+			orc_table& t = o->m.ki_binding;
+			t.nx = (int32_t)s.dims[0]; t.ny = (int32_t)s.dims[1]; t.nz = 1;
+			log_range(s.scales[0], lo, hi); set_axis(t.nx, lo, hi, true, t.x_min, t.x_step);
+			lin_range(s.scales[1], t.ny, lo, hi); set_axis(t.ny, lo, hi, false, t.y_min, t.y_step);
+			t.data = st.data();
+			std::vector<double> shells;
+			for (float v : sh.data) {
+				const double e = (double)v * unit_value(sh.unit);
+				if (e < 100) shells.push_back(e);
+			}
+			std::sort(shells.begin(), shells.end());
+			const double unit = unit_value(s.unit);
+			const nm_scale& ks = s.scales[0];
+			const double kf = ks.v.front() * unit_value(ks.unit);
+			const double kstep = std::log((ks.v.back() * unit_value(ks.unit)) / kf) / (ks.v.size() - 1);
+			double pa = 0, pb = 1;
+			if (s.scales[1].present) { pa = s.scales[1].v.front() * unit_value(s.scales[1].unit); pb = s.scales[1].v.back() * unit_value(s.scales[1].unit); }
+			const double pstep = (pb - pa) / (t.ny - 1);
+			// rewritten in place in row order while being read (as the reference does)
+			for (int32_t x = 0; x < t.nx; ++x) {
+				const double K = kf * std::exp(x * kstep);
+				for (int32_t y = 0; y < t.ny; ++y) {
+					const float P = (float)(pa + y * pstep);
+					double b = -1;
+					if (K > 100) {
+						b = (double)t2_rd(t, (float)std::log((K + 10) / 1.0), P) * unit;
+						if (b < 50 || !std::isfinite(b)) b = -1;
+					}
+					if (b < 0) {
+						const auto it = std::lower_bound(shells.rbegin(), shells.rend(), K, std::greater<double>());
+						if (it != shells.rend()) b = *it;
+					}
+					st[(size_t)x * t.ny + y] = (float)(b / 1.0);
+				}
+			}
+		}
+		if (penn) {
 		{	// q icdf (full_penn.h:348-369)
 			nm_set& s = set("/full_penn/q_icdf");
 			std::vector<float>& st = o->store[4];
@@ -793,6 +952,7 @@ extern "C" void* orc_material_load(const char* path, char* err, int errlen)
 			lin_range(s.scales[2], t.nz, lo, hi); set_axis(t.nz, lo, hi, false, t.z_min, t.z_step);
 			t.data = st.data();
 		}
+		}
 		o->m.fermi = (float)(fermi_q / 1.0);
 		{
 			auto it = f.props.find("band_gap");
@@ -808,6 +968,8 @@ extern "C" void* orc_material_load(const char* path, char* err, int errlen)
 	}
 }
 extern "C" const orc_material* orc_material_view(void* h) { return &static_cast<owned_material*>(h)->m; }
+extern "C" void orc_set_physics(uint32_t bits) { g_phys = bits; }
+extern "C" uint32_t orc_get_physics(void) { return g_phys; }
 extern "C" void orc_material_free(void* h) { delete static_cast<owned_material*>(h); }
 
 extern "C" float orc_table_get(const orc_table* t, int dims, float x, float y, float z)

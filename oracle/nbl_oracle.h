@@ -6,8 +6,8 @@
  * It restates, operation by operation and in float32 like the reference's
  * CPU build (config/config.h:13), the functions its CPU driver runs:
  * table lookups, Moller-Trumbore intersection, the octree walk, Kieft-Bosch
- * elastic, Full-Penn inelastic and boundary crossing, and the simple CPU
- * driver loop.  With the reference mt19937 generator it reproduces the
+ * elastic, Full-Penn and Kieft-Bosch inelastic and boundary crossing, with
+ * the option bools of each, and the simple CPU driver loop.  With the reference mt19937 generator it reproduces the
  * reference's detected-electron records bit for bit (checked in
  * tests/test_oracle_pin.py against oracle/_ref built from the reference).
  */
@@ -28,10 +28,24 @@ typedef struct orc_table {
 	const float* data;
 } orc_table;
 
+/* models: bit 0 Full-Penn tables (in_*) present, bit 1 Kieft-Bosch tables
+ * (ki_*: imfp 1-D, w0 ICDF 2-D, binding 2-D) present. */
 typedef struct orc_material {
 	orc_table el_imfp, el_icdf, in_imfp, in_omega, in_q, in_binding;
 	float fermi, band_gap, barrier, phonon_loss, recoil_const;
+	int32_t models;
+	orc_table ki_imfp, ki_w0, ki_binding;
 } orc_material;
+
+/* Physics selection (physics_config.h:20-46 and the option bools of the
+ * models), one bit per option, for every later event and run:
+ *   1 generate_secondary   2 acoustic_phonon_loss   4 atomic_recoil_loss
+ *   8 quantum_transmission 16 interface_refraction  32 interface_absorption
+ *   64 optical_phonon_loss 128 instantaneous_momentum 256 momentum_conservation
+ *   65536 Kieft-Bosch inelastic model instead of Full Penn.
+ * Default 1|2|4|8|16|64|128|256 (the reference's selection). */
+void orc_set_physics(uint32_t bits);
+uint32_t orc_get_physics(void);
 
 /* Linearized octree as octree_builder.h:209-248 lays it out; triangles as
  * 11 floats (material_in, material_out, r0, e1, e2). */

@@ -23,6 +23,29 @@ REF_CPU_MT = os.path.join(HERE, "_ref", "nebula_cpu_mt")
 
 TABLE_NAMES = ("el_imfp", "el_icdf", "in_imfp", "in_omega", "in_q", "in_binding")
 TABLE_DIMS = (1, 2, 1, 2, 3, 3)
+KIEFT_TABLE_NAMES = ("ki_imfp", "ki_w0", "ki_binding")
+KIEFT_TABLE_DIMS = (1, 2, 2)
+
+# Physics selection bits (nbl_oracle.h orc_set_physics; the option bools of
+# physics_config.h:20-46 and the models it names).
+PHYSICS_BITS = {"generate_secondaries": 1, "acoustic_phonon_loss": 2, "atomic_recoil_loss": 4,
+                "quantum_transmission": 8, "interface_refraction": 16, "interface_absorption": 32,
+                "optical_phonon_loss": 64, "instantaneous_momentum": 128, "momentum_conservation": 256}
+KIEFT_BIT = 65536
+PHYS_DEFAULT = 0x1DF
+
+
+def physics_bits(physics=None):
+    """Bits for a dict of nbl_physics_opts overrides (the library's names)."""
+    b = PHYS_DEFAULT
+    for k, v in (physics or {}).items():
+        if k == "inelastic_model":
+            b = (b | KIEFT_BIT) if int(v) == 1 else (b & ~KIEFT_BIT)
+        elif v:
+            b |= PHYSICS_BITS[k]
+        else:
+            b &= ~PHYSICS_BITS[k]
+    return b
 PRI_DTYPE = np.dtype([("pos", "<f4", 3), ("dir", "<f4", 3), ("E", "<f4"),
                       ("px", "<i4"), ("py", "<i4")])
 
@@ -46,7 +69,8 @@ class OrcTable(C.Structure):
 class OrcMaterial(C.Structure):
     _fields_ = [(n, OrcTable) for n in TABLE_NAMES] + [
         ("fermi", C.c_float), ("band_gap", C.c_float), ("barrier", C.c_float),
-        ("phonon_loss", C.c_float), ("recoil_const", C.c_float)]
+        ("phonon_loss", C.c_float), ("recoil_const", C.c_float), ("models", C.c_int32)] + [
+        (n, OrcTable) for n in KIEFT_TABLE_NAMES]
 
 
 class OrcGeometry(C.Structure):
@@ -89,6 +113,8 @@ def lib():
             fn.restype = C.c_int64
             fn.argtypes = [C.POINTER(OrcGeometry), C.POINTER(OrcMaterial), C.c_int, C.c_void_p,
                            C.c_int64, C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p, i64p]
+        L.orc_set_physics.argtypes = [C.c_uint32]
+        L.orc_get_physics.restype = C.c_uint32
         L.orc_simulate_mt.restype = C.c_int64
         L.orc_simulate_mt.argtypes = [C.POINTER(OrcGeometry), C.POINTER(OrcMaterial), C.c_int,
                                       C.c_void_p, C.c_int64, C.c_uint32, C.c_float, C.c_int,
@@ -165,20 +191,40 @@ class Geometry:
         return od, ot
 
 
-def event(geom, mats, kind, state, material, rng_handle, tri=-1):
+class _physics:
+    """Select the oracle's physics bits for the duration of a call."""
+
+    def __init__(self, bits):
+        self.bits = bits
+
+    def __enter__(self):
+        self.old = lib().orc_get_physics()
+        lib().orc_set_physics(self.bits)
+
+    def __exit__(self, *a):
+        lib().orc_set_physics(self.old)
+
+
+def event(geom, mats, kind, state, material, rng_handle, tri=-1, phys=PHYS_DEFAULT):
     """One event through the oracle; returns (state, material, status, se or None)."""
     st = np.ascontiguousarray(state, np.float32).copy()
     m = np.array([material], np.int32)
     se = np.zeros(7, np.float32)
     status = np.zeros(1, np.int32)
     arr = materials_array(mats)
-    n = lib().orc_event(C.byref(geom.s) if geom is not None else None, arr, len(mats), kind, tri,
-                        rng_handle, _p(st, f32p), _p(m, i32p), _p(se, f32p), _p(status, i32p))
+    with _physics(phys):
+        n = lib().orc_event(C.byref(geom.s) if geom is not None else None, arr, len(mats), kind, tri,
+                            rng_handle, _p(st, f32p), _p(m, i32p), _p(se, f32p), _p(status, i32p))
     return st, int(m[0]), int(status[0]), (se if n else None)
 
 
-def simulate(geom, mats, pri, seed, energy_threshold=0.0, threads=1, max_records=None):
+def simulate(geom, mats, pri, seed, energy_threshold=0.0, threads=1, max_records=None, phys=PHYS_DEFAULT):
     """Run the oracle driver loop; returns (records, n_total, n_events)."""
+    with _physics(phys):
+        return _simulate(geom, mats, pri, seed, energy_threshold, threads, max_records)
+
+
+def _simulate(geom, mats, pri, seed, energy_threshold, threads, max_records):
     pri = np.ascontiguousarray(pri, PRI_DTYPE)
     cap = max_records if max_records is not None else max(16, 4 * len(pri) + 1024)
     out = np.zeros(cap, PRI_DTYPE)
@@ -224,11 +270,11 @@ def ref():
         L.ref_material_constants.argtypes = [C.c_void_p, f32p]
         L.ref_table_lookup.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int64, f32p, f32p, f32p, f32p]
         L.ref_event.restype = C.c_int
-        L.ref_event.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int32,
+        L.ref_event.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_uint32, C.c_int, C.c_int32,
                                 C.c_uint32, f32p, i32p, f32p, C.c_int, i32p]
         L.ref_simulate.restype = C.c_int64
-        L.ref_simulate.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_void_p, C.c_int64,
-                                   C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p, i64p]
+        L.ref_simulate.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_uint32, C.c_void_p,
+                                   C.c_int64, C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p, i64p]
         _ref = L
     return _ref
 
@@ -278,7 +324,7 @@ class RefMaterial:
             raise RuntimeError(L.ref_last_error().decode())
 
     def table(self, name):
-        which = TABLE_NAMES.index(name)
+        which = (TABLE_NAMES + KIEFT_TABLE_NAMES).index(name)
         shape = np.zeros(3, np.int32)
         scale = np.zeros(6, np.float32)
         ref().ref_material_table_shape(self.h, which, _p(shape, i32p), _p(scale, f32p))
@@ -297,7 +343,7 @@ class RefMaterial:
         y = np.ascontiguousarray(np.zeros(n) if y is None else y, np.float32)
         z = np.ascontiguousarray(np.zeros(n) if z is None else z, np.float32)
         out = np.empty(n, np.float32)
-        ref().ref_table_lookup(self.h, TABLE_NAMES.index(name), int(rounddown), n, _p(x, f32p),
+        ref().ref_table_lookup(self.h, (TABLE_NAMES + KIEFT_TABLE_NAMES).index(name), int(rounddown), n, _p(x, f32p),
                                _p(y, f32p), _p(z, f32p), _p(out, f32p))
         return out
 
@@ -306,24 +352,26 @@ class RefMaterial:
             _ref.ref_material_free(self.h)
 
 
-def ref_event(geom, mats, kind, state, material, seed, tri=-1):
+def ref_event(geom, mats, kind, state, material, seed, tri=-1, phys=PHYS_DEFAULT):
     st = np.ascontiguousarray(state, np.float32).copy()
     m = np.array([material], np.int32)
     se = np.zeros(7 * 4, np.float32)
     status = np.zeros(1, np.int32)
     hs = (C.c_void_p * len(mats))(*[x.h for x in mats])
-    n = ref().ref_event(geom.h if geom is not None else None, hs, len(mats), kind, tri, seed,
+    n = ref().ref_event(geom.h if geom is not None else None, hs, len(mats), phys, kind, tri, seed,
                         _p(st, f32p), _p(m, i32p), _p(se, f32p), 4, _p(status, i32p))
     return st, int(m[0]), int(status[0]), (se[:7].copy() if n else None)
 
 
-def ref_simulate(geom, mats, pri, seed, energy_threshold=0.0, max_records=None):
+def ref_simulate(geom, mats, pri, seed, energy_threshold=0.0, max_records=None, phys=PHYS_DEFAULT):
     pri = np.ascontiguousarray(pri, PRI_DTYPE)
     cap = max_records if max_records is not None else max(16, 4 * len(pri) + 1024)
     out = np.zeros(cap, PRI_DTYPE)
     tot = C.c_int64(0)
     ev = C.c_int64(0)
     hs = (C.c_void_p * len(mats))(*[x.h for x in mats])
-    n = ref().ref_simulate(geom.h, hs, len(mats), pri.ctypes.data, len(pri), seed, energy_threshold,
+    n = ref().ref_simulate(geom.h, hs, len(mats), phys, pri.ctypes.data, len(pri), seed, energy_threshold,
                            out.ctypes.data, cap, C.byref(tot), C.byref(ev))
+    if n < 0:
+        raise RuntimeError(ref().ref_last_error().decode())
     return out[:n], tot.value, ev.value

@@ -14,14 +14,17 @@
  *   ref_propagate    octree<false>::propagate (geometry/octree.inl:33-192)
  *   ref_material_*   material<scatter_physics<false>>(hdf5_file)
  *                    (core/material.inl:13-18): full_penn::create,
- *                    kieft_elastic::create; table dumps and table lookups
- *   ref_event        one scatter (scatter_list::execute) or one boundary
+ *                    kieft_elastic::create, kieft_inelastic::create; table
+ *                    dumps and table lookups
+ *   ref_event        one scatter (the model's execute) or one boundary
  *                    crossing (boundary_intersect::execute) on one electron
  *                    held by the reference cpu_particle_manager, with the
- *                    reference mt19937 generator seeded by the caller
+ *                    reference mt19937 generator seeded by the caller, for
+ *                    any combination of the models' option bools
  *   ref_simulate     the cpu_mt_main.cpp sim_loop (lines 167-201) run on ONE
  *                    thread with one seed, so the run is deterministic:
- *                    push one primary, simulate_to_end, flush_detected.
+ *                    push one primary, simulate_to_end, flush_detected; for
+ *                    the reference's physics selection and three others.
  *
  * Private/protected members are opened with the preprocessor so that the
  * tables can be dumped and the driver's init/intersect/scatter steps counted.
@@ -160,76 +163,150 @@ int ref_in_domain(void* h, const float* pos)
 }
 
 /* ---------------------------------------------------------------- materials */
+/* A material handle keeps the material file (the in-memory stand-in) and
+ * creates the reference's objects from it: the default-physics material
+ * (when the file carries Full-Penn tables) and, on demand, the scatter
+ * models with other option bools or the Kieft-Bosch inelastic model. */
+namespace {
+using kieft_default_t = nbl::scatter::kieft_inelastic<false>;
+struct ref_material
+{
+	nbl::hdf5_file file;
+	bool penn = false, kieft = false;
+	std::unique_ptr<material_t> def;
+	std::unique_ptr<kieft_default_t> ki;
+	float barrier = 0;
+	explicit ref_material(const char* path) : file(path)
+	{
+		penn = file.exists("/full_penn");
+		kieft = file.exists("/inelastic_kieft");
+		if (penn)
+			def.reset(new material_t(file));
+		if (kieft)
+			ki.reset(new kieft_default_t(kieft_default_t::create(file)));
+		barrier = static_cast<float>(file.get_property_quantity("barrier") / nbl::units::eV);
+	}
+	~ref_material() { if (ki) kieft_default_t::destroy(*ki); }
+};
+}
+
 void* ref_material_load(const char* path)
 {
 	try {
-		return new material_t(nbl::hdf5_file(path));
+		return new ref_material(path);
 	} catch (std::exception const & e) {
 		g_err = e.what();
 		return nullptr;
 	}
 }
-void ref_material_free(void* h) { delete static_cast<material_t*>(h); }
+void ref_material_free(void* h) { delete static_cast<ref_material*>(h); }
 
-/* Table geometry: which = 0 el_imfp, 1 el_icdf, 2 in_imfp, 3 in_omega, 4 in_q, 5 in_binding.
+/* Table geometry: which = 0 el_imfp, 1 el_icdf, 2 in_imfp, 3 in_omega, 4 in_q,
+ * 5 in_binding (Full Penn), 6 ki_imfp, 7 ki_w0, 8 ki_binding (Kieft-Bosch).
  * shape[3] (1 for absent axes), scale[6] (x_min, x_step, y_min, y_step, z_min, z_step). */
-static void table_info(material_t* m, int which, int32_t* shape, float* scale, const float** data, int64_t* pitch_floats)
+extern "C++" {
+namespace {
+struct table_desc { int32_t* shape; float* scale; const float** data; int64_t* pitch; };
+template<class T> void desc1(const T& t, table_desc d)
 {
-	auto& inel = nbl::tuple::get<0>(*m);
-	auto& el = nbl::tuple::get<1>(*m);
+	d.shape[0] = t._n; d.scale[0] = t._x_min; d.scale[1] = t._x_step; *d.data = t._data;
+}
+template<class T> void desc2(const T& t, table_desc d)
+{
+	d.shape[0] = t._width; d.shape[1] = t._height;
+	d.scale[0] = t._x_min; d.scale[1] = t._x_step; d.scale[2] = t._y_min; d.scale[3] = t._y_step;
+	*d.data = t._data; *d.pitch = (int64_t)(t._pitch / sizeof(float));
+}
+template<class T> void desc3(const T& t, table_desc d)
+{
+	d.shape[0] = t._width; d.shape[1] = t._height; d.shape[2] = t._depth;
+	d.scale[0] = t._x_min; d.scale[1] = t._x_step; d.scale[2] = t._y_min; d.scale[3] = t._y_step;
+	d.scale[4] = t._z_min; d.scale[5] = t._z_step;
+	*d.data = t._data; *d.pitch = (int64_t)(t._pitch / sizeof(float));
+}
+}
+}  // extern "C++"
+
+static void table_info(ref_material* rm, int which, int32_t* shape, float* scale, const float** data, int64_t* pitch_floats)
+{
 	shape[0] = shape[1] = shape[2] = 1;
 	for (int k = 0; k < 6; ++k) scale[k] = 0;
 	*pitch_floats = 0;
+	*data = nullptr;
+	const table_desc d{ shape, scale, data, pitch_floats };
+	if (which >= 6) {
+		if (!rm->ki) throw std::runtime_error("no Kieft-Bosch tables");
+		if (which == 6) desc1(rm->ki->_log_imfp_table, d);
+		else if (which == 7) desc2(rm->ki->_log_icdf_table, d);
+		else desc2(rm->ki->_ionisation_table, d);
+		return;
+	}
+	if (!rm->def) {
+		if (which > 1) throw std::runtime_error("no Full-Penn tables");
+		// elastic tables of a Kieft-Bosch-only file
+		static thread_local std::unique_ptr<nbl::scatter::kieft_elastic<false>> el;
+		el.reset(new nbl::scatter::kieft_elastic<false>(nbl::scatter::kieft_elastic<false>::create(rm->file)));
+		if (which == 0) desc1(el->_log_imfp_table, d); else desc2(el->_icdf_table, d);
+		return;
+	}
+	auto& inel = nbl::tuple::get<0>(*rm->def);
+	auto& el = nbl::tuple::get<1>(*rm->def);
 	switch (which) {
-	case 0: shape[0] = el._log_imfp_table._n; scale[0] = el._log_imfp_table._x_min; scale[1] = el._log_imfp_table._x_step; *data = el._log_imfp_table._data; break;
-	case 2: shape[0] = inel._log_imfp_table._n; scale[0] = inel._log_imfp_table._x_min; scale[1] = inel._log_imfp_table._x_step; *data = inel._log_imfp_table._data; break;
-	case 1: case 3: {
-		auto& t = which == 1 ? el._icdf_table : inel._log_omega_icdf_table;
-		shape[0] = t._width; shape[1] = t._height;
-		scale[0] = t._x_min; scale[1] = t._x_step; scale[2] = t._y_min; scale[3] = t._y_step;
-		*data = t._data; *pitch_floats = (int64_t)(t._pitch / sizeof(float)); break; }
-	default: {
-		auto& t = which == 4 ? inel._q_icdf_table : inel._ionisation_table;
-		shape[0] = t._width; shape[1] = t._height; shape[2] = t._depth;
-		scale[0] = t._x_min; scale[1] = t._x_step; scale[2] = t._y_min; scale[3] = t._y_step;
-		scale[4] = t._z_min; scale[5] = t._z_step;
-		*data = t._data; *pitch_floats = (int64_t)(t._pitch / sizeof(float)); break; }
+	case 0: desc1(el._log_imfp_table, d); break;
+	case 2: desc1(inel._log_imfp_table, d); break;
+	case 1: desc2(el._icdf_table, d); break;
+	case 3: desc2(inel._log_omega_icdf_table, d); break;
+	case 4: desc3(inel._q_icdf_table, d); break;
+	default: desc3(inel._ionisation_table, d); break;
 	}
 }
 
 void ref_material_table_shape(void* h, int which, int32_t* shape, float* scale)
 {
 	const float* data; int64_t pitch;
-	table_info(static_cast<material_t*>(h), which, shape, scale, &data, &pitch);
+	table_info(static_cast<ref_material*>(h), which, shape, scale, &data, &pitch);
 }
 
 /* Dense row-major copy of a table (rows are contiguous on the CPU). */
 void ref_material_table_data(void* h, int which, float* out)
 {
 	int32_t shape[3]; float scale[6]; const float* data; int64_t pitch;
-	table_info(static_cast<material_t*>(h), which, shape, scale, &data, &pitch);
+	table_info(static_cast<ref_material*>(h), which, shape, scale, &data, &pitch);
 	std::memcpy(out, data, sizeof(float) * (size_t)shape[0] * shape[1] * shape[2]);
 }
 
 /* [fermi, band_gap, barrier, phonon_loss, recoil_const] */
 void ref_material_constants(void* h, float* out)
 {
-	auto* m = static_cast<material_t*>(h);
-	auto& inel = nbl::tuple::get<0>(*m);
-	auto& el = nbl::tuple::get<1>(*m);
-	out[0] = inel._fermi; out[1] = inel._band_gap; out[2] = m->barrier;
+	auto* rm = static_cast<ref_material*>(h);
+	auto el = nbl::scatter::kieft_elastic<false>::create(rm->file);
+	if (rm->def) {
+		auto& inel = nbl::tuple::get<0>(*rm->def);
+		out[0] = inel._fermi; out[1] = inel._band_gap;
+	} else {
+		out[0] = rm->ki->_fermi; out[1] = rm->ki->_band_gap;
+	}
+	out[2] = rm->barrier;
 	out[3] = el._phonon_loss; out[4] = el._recoil_const;
+	nbl::scatter::kieft_elastic<false>::destroy(el);
 }
 
 /* Table lookups through the reference table classes (get / get_rounddown). */
 void ref_table_lookup(void* h, int which, int rounddown, int64_t n, const float* x, const float* y,
 	const float* z, float* out)
 {
-	auto* m = static_cast<material_t*>(h);
-	auto& inel = nbl::tuple::get<0>(*m);
-	auto& el = nbl::tuple::get<1>(*m);
+	auto* rm = static_cast<ref_material*>(h);
 	for (int64_t i = 0; i < n; ++i)
 	{
+		if (which >= 6) {
+			auto& k = *rm->ki;
+			if (which == 6) out[i] = k._log_imfp_table.get(x[i]);
+			else if (which == 7) out[i] = rounddown ? k._log_icdf_table.get_rounddown(x[i], y[i]) : k._log_icdf_table.get(x[i], y[i]);
+			else out[i] = rounddown ? k._ionisation_table.get_rounddown(x[i], y[i]) : k._ionisation_table.get(x[i], y[i]);
+			continue;
+		}
+		auto& inel = nbl::tuple::get<0>(*rm->def);
+		auto& el = nbl::tuple::get<1>(*rm->def);
 		switch (which) {
 		case 0: out[i] = el._log_imfp_table.get(x[i]); break;
 		case 2: out[i] = inel._log_imfp_table.get(x[i]); break;
@@ -242,20 +319,100 @@ void ref_table_lookup(void* h, int which, int rounddown, int64_t n, const float*
 }
 
 /* ------------------------------------------------------------------- events */
+/* Physics bits (the oracle's numbering): 1 generate_secondary, 2
+ * acoustic_phonon_loss, 4 atomic_recoil_loss, 8 quantum_transmission, 16
+ * interface_refraction, 32 interface_absorption, 64 optical_phonon_loss, 128
+ * instantaneous_momentum, 256 momentum_conservation, 65536 Kieft-Bosch
+ * inelastic model.  Each bit selects the reference template argument of the
+ * same name; one instantiation per combination. */
+extern "C++" {
+namespace {
+template<class T, class PM>
+void run_scatter(ref_material* rm, PM& pm, nbl::util::random_generator<false>& rng)
+{
+	T obj = T::create(rm->file);
+	obj.execute(pm, 0, rng);
+	T::destroy(obj);
+}
+
+template<class PM>
+void elastic_dispatch(uint32_t b, ref_material* rm, PM& pm, nbl::util::random_generator<false>& rng)
+{
+	using namespace nbl::scatter;
+	switch ((b >> 1) & 3) {
+	case 0: run_scatter<kieft_elastic<false, false, false>>(rm, pm, rng); break;
+	case 1: run_scatter<kieft_elastic<false, true, false>>(rm, pm, rng); break;
+	case 2: run_scatter<kieft_elastic<false, false, true>>(rm, pm, rng); break;
+	default: run_scatter<kieft_elastic<false, true, true>>(rm, pm, rng); break;
+	}
+}
+
+template<bool gen, class PM>
+void kieft_dispatch2(uint32_t b, ref_material* rm, PM& pm, nbl::util::random_generator<false>& rng)
+{
+	using namespace nbl::scatter;
+	switch ((((b >> 6) & 1) << 2) | (((b >> 7) & 1) << 1) | ((b >> 8) & 1)) {
+	case 0: run_scatter<kieft_inelastic<false, false, gen, false, false>>(rm, pm, rng); break;
+	case 1: run_scatter<kieft_inelastic<false, false, gen, false, true>>(rm, pm, rng); break;
+	case 2: run_scatter<kieft_inelastic<false, false, gen, true, false>>(rm, pm, rng); break;
+	case 3: run_scatter<kieft_inelastic<false, false, gen, true, true>>(rm, pm, rng); break;
+	case 4: run_scatter<kieft_inelastic<false, true, gen, false, false>>(rm, pm, rng); break;
+	case 5: run_scatter<kieft_inelastic<false, true, gen, false, true>>(rm, pm, rng); break;
+	case 6: run_scatter<kieft_inelastic<false, true, gen, true, false>>(rm, pm, rng); break;
+	default: run_scatter<kieft_inelastic<false, true, gen, true, true>>(rm, pm, rng); break;
+	}
+}
+
+template<class PM>
+void inelastic_dispatch(uint32_t b, ref_material* rm, PM& pm, nbl::util::random_generator<false>& rng)
+{
+	using namespace nbl::scatter;
+	if (b & 65536) {
+		if (b & 1) kieft_dispatch2<true>(b, rm, pm, rng);
+		else kieft_dispatch2<false>(b, rm, pm, rng);
+	} else {
+		if (b & 1) run_scatter<full_penn<false, true>>(rm, pm, rng);
+		else run_scatter<full_penn<false, false>>(rm, pm, rng);
+	}
+}
+
+template<class MM, class PM>
+void boundary_dispatch(uint32_t b, MM& mm, PM& pm, nbl::util::random_generator<false>& rng)
+{
+	switch ((b >> 3) & 7) {
+	case 0: { boundary_intersect<false, false, false> i; i.execute(mm, pm, 0, rng); break; }
+	case 1: { boundary_intersect<true, false, false> i; i.execute(mm, pm, 0, rng); break; }
+	case 2: { boundary_intersect<false, true, false> i; i.execute(mm, pm, 0, rng); break; }
+	case 3: { boundary_intersect<true, true, false> i; i.execute(mm, pm, 0, rng); break; }
+	case 4: { boundary_intersect<false, false, true> i; i.execute(mm, pm, 0, rng); break; }
+	case 5: { boundary_intersect<true, false, true> i; i.execute(mm, pm, 0, rng); break; }
+	case 6: { boundary_intersect<false, true, true> i; i.execute(mm, pm, 0, rng); break; }
+	default: { boundary_intersect<true, true, true> i; i.execute(mm, pm, 0, rng); break; }
+	}
+}
+
+// Material list for the managers: the boundary step only reads `barrier`, so
+// a material made of the elastic model alone serves every file.
+using bmat_phys = scatter_list<nbl::scatter::kieft_elastic<false>>;
+using bdriver_t = nbl::drivers::simple_cpu_driver<bmat_phys, intersect_t, geometry_t>;
+}
+}  // extern "C++"
+
 /* Electron in/out: [pos3, dir3, E] plus material index.
  * kind: 1 inelastic, 2 elastic (scatter_list order), 3 boundary crossing on
  * triangle `tri` of geometry `gh`.  The generator is the reference
- * random_generator<false> seeded with `seed`.
+ * random_generator<false> seeded with `seed`; `phys` selects the models and
+ * options (bits above).
  * Returns the number of secondaries written to se_out (7 floats each) and sets
  * *status: 0 running, 1 detected, 2 terminated. */
-int ref_event(void* gh, void** mats, int n_mat, int kind, int32_t tri, uint32_t seed,
+int ref_event(void* gh, void** mats, int n_mat, uint32_t phys, int kind, int32_t tri, uint32_t seed,
 	float* state, int32_t* material, float* se_out, int max_se, int32_t* status)
 {
-	std::vector<material_t> materials;
+	std::vector<::material<bmat_phys>> materials;
 	for (int i = 0; i < n_mat; ++i)
-		materials.push_back(*static_cast<material_t*>(mats[i]));
-	using pm_t = driver_t::particle_manager_t;
-	using mm_t = driver_t::material_manager_t;
+		materials.emplace_back(static_cast<ref_material*>(mats[i])->file);
+	using pm_t = bdriver_t::particle_manager_t;
+	using mm_t = bdriver_t::material_manager_t;
 	pm_t pm = pm_t::create();
 	mm_t mm = mm_t::create(materials);
 	particle p{ { state[0], state[1], state[2] }, { state[3], state[4], state[5] }, state[6] };
@@ -268,12 +425,13 @@ int ref_event(void* gh, void** mats, int n_mat, int kind, int32_t tri, uint32_t 
 		auto* g = static_cast<ref_geometry*>(gh);
 		pm.particles[0].last_triangle = g->oct._triangles + tri;
 		pm.particles[0].status = pm_t::INTERSECT_EVENT;
-		intersect_t isect;
-		isect.execute(mm, pm, 0, rng);
+		boundary_dispatch(phys, mm, pm, rng);
 	}
 	else
 	{
-		mm[*material].execute((uint8_t)kind, pm, 0, rng);
+		auto* rm = static_cast<ref_material*>(mats[*material]);
+		if (kind == 1) inelastic_dispatch(phys, rm, pm, rng);
+		else elastic_dispatch(phys, rm, pm, rng);
 	}
 	particle q = pm[0];
 	state[0] = q.pos.x; state[1] = q.pos.y; state[2] = q.pos.z;
@@ -300,16 +458,20 @@ int ref_event(void* gh, void** mats, int n_mat, int kind, int32_t tri, uint32_t 
  * and flush detected electrons as 36-byte records (pixel = the primary's).
  * Returns the number of records (capped at max_records; *n_total gets the
  * uncapped count). */
-int64_t ref_simulate(void* gh, void** mats, int n_mat, const void* pri_records, int64_t n_pri,
+extern "C++" {
+namespace {
+template<class Phys, class Isect>
+int64_t simulate_impl(void* gh, void** mats, int n_mat, const void* pri_records, int64_t n_pri,
 	uint32_t seed, float energy_threshold, void* out_records, int64_t max_records,
 	int64_t* n_total, int64_t* n_events)
 {
+	using drv_t = nbl::drivers::simple_cpu_driver<Phys, Isect, geometry_t>;
 	auto* g = static_cast<ref_geometry*>(gh);
-	std::vector<material_t> materials;
+	std::vector<material<Phys>> materials;
 	for (int i = 0; i < n_mat; ++i)
-		materials.push_back(*static_cast<material_t*>(mats[i]));
-	intersect_t inter;
-	driver_t d(g->oct, inter, materials, energy_threshold, seed);
+		materials.emplace_back(static_cast<ref_material*>(mats[i])->file);
+	Isect inter;
+	drv_t d(g->oct, inter, materials, energy_threshold, seed);
 	int64_t written = 0, total = 0, events = 0;
 	const char* in = static_cast<const char*>(pri_records);
 	char* out = static_cast<char*>(out_records);
@@ -329,12 +491,6 @@ int64_t ref_simulate(void* gh, void** mats, int n_mat, const void* pri_records, 
 				d.intersect(idx);
 				d.scatter(idx);
 				++events;
-				if (std::getenv("NBL_TRACE")) {
-					auto const & q = d._particles.particles[idx];
-					std::fprintf(stderr, "R %zu %d %d %.9g %.9g %.9g %.9g %.9g %.9g %.9g\n", idx, (int)q.status, q.current_material,
-						q.particle_data.pos.x, q.particle_data.pos.y, q.particle_data.pos.z,
-						q.particle_data.dir.x, q.particle_data.dir.y, q.particle_data.dir.z, q.particle_data.kin_energy);
-				}
 			}
 		}
 		d.flush_detected([&](particle q, uint32_t) {
@@ -351,6 +507,43 @@ int64_t ref_simulate(void* gh, void** mats, int n_mat, const void* pri_records, 
 	*n_total = total;
 	*n_events = events;
 	return written;
+}
+}
+}  // extern "C++"
+
+/* Physics presets with a compiled driver (bits as for ref_event):
+ *   0x1DF      the reference's selection (physics_config.h)
+ *   0x101DF    Kieft-Bosch inelastic, every option on
+ *   0x1E1      Full Penn; no phonon or recoil loss; classical transmission,
+ *              no refraction, empirical absorption
+ *   0x1001F    Kieft-Bosch without optical-phonon loss, instantaneous
+ *              momentum or momentum conservation
+ * Any other value returns -1. */
+int64_t ref_simulate(void* gh, void** mats, int n_mat, uint32_t phys, const void* pri_records, int64_t n_pri,
+	uint32_t seed, float energy_threshold, void* out_records, int64_t max_records,
+	int64_t* n_total, int64_t* n_events)
+{
+	using namespace nbl::scatter;
+	switch (phys) {
+	case 0x1DF:
+		return simulate_impl<scatter_physics<false>, intersect_t>(gh, mats, n_mat, pri_records, n_pri, seed,
+			energy_threshold, out_records, max_records, n_total, n_events);
+	case 0x101DF:
+		return simulate_impl<scatter_list<kieft_inelastic<false, true, true, true, true>, kieft_elastic<false, true, true>>,
+			intersect_t>(gh, mats, n_mat, pri_records, n_pri, seed, energy_threshold, out_records, max_records,
+			n_total, n_events);
+	case 0x1E1:
+		return simulate_impl<scatter_list<full_penn<false, true>, kieft_elastic<false, false, false>>,
+			boundary_intersect<false, false, true>>(gh, mats, n_mat, pri_records, n_pri, seed, energy_threshold,
+			out_records, max_records, n_total, n_events);
+	case 0x1001F:
+		return simulate_impl<scatter_list<kieft_inelastic<false, false, true, false, false>, kieft_elastic<false, true, true>>,
+			intersect_t>(gh, mats, n_mat, pri_records, n_pri, seed, energy_threshold, out_records, max_records,
+			n_total, n_events);
+	default:
+		g_err = "physics preset not compiled in the harness";
+		return -1;
+	}
 }
 
 } // extern "C"

@@ -35,8 +35,10 @@ def inputs(tmp_path_factory):
     geometry.write_tri(str(d / "grating.tri"), gr)
     nmat.write(str(d / "si.nmat"), materials.build_raw_material(materials.silicon()))
     nmat.write(str(d / "pmma.nmat"), materials.build_raw_material(materials.pmma()))
+    nmat.write(str(d / "si_kieft.nmat"), materials.build_raw_material(materials.silicon(), inelastic="kieft"))
+    nmat.write(str(d / "pmma_kieft.nmat"), materials.build_raw_material(materials.pmma(), inelastic="kieft"))
     out["dir"] = str(d)
-    for k in ("slab.tri", "grating.tri", "si.nmat", "pmma.nmat"):
+    for k in ("slab.tri", "grating.tri", "si.nmat", "pmma.nmat", "si_kieft.nmat", "pmma_kieft.nmat"):
         out[k] = str(d / k)
     return out
 
