@@ -201,7 +201,9 @@ typedef struct nbl_params {
 	uint32_t max_events;         /* per-electron flight budget; 0: 1 << 22 */
 	void* stream;                /* cudaStream_t to run on; NULL: a library-owned stream */
 	nbl_physics_opts physics;
-	int32_t adjoint;             /* 1: accumulate score functions (see nbl_adjoint_*) */
+	int32_t adjoint;             /* 1: accumulate score functions (see nbl_sim_gradients) */
+	float adjoint_w_step;        /* eV; > 0: work-function derivative by a shifted replay
+	                                (see nbl_sim_gradients); 0: transmission score only */
 } nbl_params;
 void nbl_params_defaults(nbl_params* p);
 
@@ -258,18 +260,31 @@ void nbl_sim_destroy(nbl_sim* s);
  * are fixed at material load). */
 nbl_status nbl_sim_set_theta(nbl_sim* s, const float* theta, int32_t n);
 nbl_status nbl_sim_get_theta(nbl_sim* s, float* theta, int32_t n);
-/* Score-function (likelihood-ratio) gradients of the per-pixel SE and BSE
- * counts: a simulation created with params.adjoint = 1 replays each primary
- * with the same random numbers as an adjoint = 0 run with the same seed
- * (identical trajectories and tallies) while every electron carries
- * d log p(path)/d theta -- its own free flights (chosen event and survival
- * densities) and boundary transmissions, plus its ancestry up to its creation
- * -- and every detection adds it to its pixel.  Output: FP64 sums,
+/* Gradients of the per-pixel SE and BSE counts with respect to theta.  A
+ * simulation created with params.adjoint = 1 replays each primary with the
+ * same random numbers as an adjoint = 0 run with the same seed while every
+ * electron carries the score d log p(path)/d theta of its own free flights
+ * (chosen event and survival densities) and of its ancestry up to its
+ * creation; every detection adds it to its pixel.  Output: FP64 sums,
  * [tally_ny][tally_nx][6] each; divide by the primaries of a pixel for the
- * yield gradient.  The work-function derivative is the score of the
- * transmission probability only: its deterministic effects on the crossing
- * (energy shift, refraction) are not differentiated. */
-nbl_status nbl_sim_gradients(nbl_sim* s, double* grad_se, double* grad_bse);
+ * yield gradient.
+ *
+ * The mean-free-path scales enter the path density only: their entries are
+ * score-function (likelihood-ratio) estimates.  The work function also moves
+ * the crossing deterministically (energy shift, refraction, the escape
+ * threshold), which a score cannot carry.  So:
+ *   adjoint_w_step = 0: the work-function entries are the score of the
+ *     transmission probability alone (the replay's tallies equal the
+ *     forward run's; `forward` may be NULL);
+ *   adjoint_w_step = h > 0: each primary's cascade is replayed with the work
+ *     functions shifted by h * r_m, r_m = +-1 drawn per primary and material,
+ *     on the same random numbers; the work-function entries are
+ *     (sum of r_m over the replay's detections - the same sum over `forward`'s)
+ *     / h, `forward` being the adjoint = 0 run with the same seed, primaries
+ *     and tally grid.  This is a central difference in expectation (the odd
+ *     moments of r vanish), in the same single replay.
+ * No counterpart in the reference. */
+nbl_status nbl_sim_gradients(nbl_sim* s, const nbl_sim* forward, double* grad_se, double* grad_bse);
 
 /* ------------------------------------------------------------ batched runs */
 /* Many scan jobs -- each with its own geometry, primaries and seed -- fed

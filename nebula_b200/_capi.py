@@ -70,7 +70,7 @@ class Params(C.Structure):
                 ("iterations_per_graph", C.c_uint32), ("record_capacity", C.c_uint32),
                 ("tally_nx", C.c_int32), ("tally_ny", C.c_int32), ("hist_bins", C.c_int32),
                 ("hist_emax", C.c_float), ("max_events", C.c_uint32), ("stream", C.c_void_p),
-                ("physics", PhysicsOpts), ("adjoint", C.c_int32)]
+                ("physics", PhysicsOpts), ("adjoint", C.c_int32), ("adjoint_w_step", C.c_float)]
 
 
 class BatchJob(C.Structure):
@@ -130,7 +130,7 @@ _DECLS = [
     ("nbl_sim_set_seed", C.c_int, [C.c_void_p, C.c_uint64]),
     ("nbl_sim_set_theta", C.c_int, [C.c_void_p, f32p, C.c_int32]),
     ("nbl_sim_get_theta", C.c_int, [C.c_void_p, f32p, C.c_int32]),
-    ("nbl_sim_gradients", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("nbl_sim_gradients", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("nbl_sim_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_destroy", None, [C.c_void_p]),
     ("nbl_batch_params_defaults", None, [C.POINTER(BatchParams)]),

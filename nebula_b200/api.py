@@ -230,7 +230,8 @@ class Simulation:
 
     def __init__(self, geometry, materials, capacity=1 << 20, seed=0x78C7E39B, energy_threshold=0.0, device=0,
                  tally=(0, 0), hist_bins=200, hist_emax=1000.0, record_capacity=0, block_size=0, grid_size=0,
-                 iterations_per_graph=0, max_events=0, adjoint=False, stream=None, physics=None):
+                 iterations_per_graph=0, max_events=0, adjoint=False, stream=None, physics=None,
+                 adjoint_w_step=0.0):
         p = _capi.Params()
         lib().nbl_params_defaults(C.byref(p))
         p.physics = physics_options(physics)
@@ -247,6 +248,7 @@ class Simulation:
         p.iterations_per_graph = iterations_per_graph
         p.max_events = max_events
         p.adjoint = int(bool(adjoint))
+        p.adjoint_w_step = adjoint_w_step
         p.stream = stream
         self.params = p
         self.tally = tuple(tally)
@@ -334,13 +336,16 @@ class Simulation:
         check(lib().nbl_sim_get_theta(self._h, _fp(t), len(t)))
         return t
 
-    def gradients(self):
+    def gradients(self, forward=None):
         """Per-pixel FP64 sums of d(SE count)/d theta and d(BSE count)/d
-        theta, shape (ny, nx, 6) each (adjoint simulations only)."""
+        theta, shape (ny, nx, 6) each (adjoint simulations only).  With
+        ``adjoint_w_step > 0`` the work-function entries need ``forward``,
+        the adjoint=False run of the same primaries and seed."""
         nx, ny = self.tally
         gs = np.zeros((ny, nx, 6), np.float64)
         gb = np.zeros((ny, nx, 6), np.float64)
-        check(lib().nbl_sim_gradients(self._h, gs.ctypes.data_as(C.POINTER(C.c_double)),
+        check(lib().nbl_sim_gradients(self._h, forward._h if forward is not None else None,
+                                      gs.ctypes.data_as(C.POINTER(C.c_double)),
                                       gb.ctypes.data_as(C.POINTER(C.c_double))))
         return gs, gb
 

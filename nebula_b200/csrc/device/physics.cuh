@@ -321,7 +321,8 @@ enum : int { ST_RUNNING = 0, ST_DETECTED = 1, ST_TERMINATED = 2 };
 struct BoundaryScore { float d_in, d_out; int mat_in, mat_out; };
 
 template<class R> __device__ __forceinline__ int boundary_event(const DevTriangle& T, const DevMaterial* __restrict__ mats,
-	Electron& p, int& material, R& rng, BoundaryScore* score = nullptr, uint32_t ph = PH_DEFAULT)
+	Electron& p, int& material, R& rng, BoundaryScore* score = nullptr, uint32_t ph = PH_DEFAULT,
+	const float* dbar = nullptr)
 {
 	const V3 nd = vnormalised(p.dir);
 	const V3 n = vnormalised(v3(T.nx, T.ny, T.nz));
@@ -338,9 +339,10 @@ template<class R> __device__ __forceinline__ int boundary_event(const DevTriangl
 	default: break;
 	}
 	if (score) { score->mat_in = min_; score->mat_out = mout; }
+	// `dbar` (adjoint replay): barrier shifts of materials 0 and 1
 	float dU = 0.0f;
-	if (min_ >= 0) dU = fs(dU, mats[min_].barrier);
-	if (mout >= 0) dU = fa(dU, mats[mout].barrier);
+	if (min_ >= 0) dU = fs(dU, (dbar && min_ < 2) ? fa(mats[min_].barrier, dbar[min_]) : mats[min_].barrier);
+	if (mout >= 0) dU = fa(dU, (dbar && mout < 2) ? fa(mats[mout].barrier, dbar[mout]) : mats[mout].barrier);
 	const float Ec2 = fm(fm(p.E, c), c);
 	float g = 0.0f;                                          // d log P(outcome) / d dU
 	if (fa(Ec2, dU) > 0.0f) {

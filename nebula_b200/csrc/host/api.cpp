@@ -70,7 +70,7 @@ struct nbl_sim {
 	DeviceMaterials mats;
 	DevBuf queues[2][N_QUEUES][6];
 	DevBuf spill[6];
-	DevBuf ctrl, counters, detected, n_detected, se_img, bse_img, hist, grad_se, grad_bse;
+	DevBuf ctrl, counters, detected, n_detected, se_img, bse_img, hist, grad_se, grad_bse, wsign_se, wsign_bse;
 	DevBuf primaries;
 	uint64_t pri_cap = 0, n_pri = 0;
 	StepParams sp{};
@@ -221,6 +221,8 @@ struct nbl_sim {
 		if (hist.p) CU(cudaMemsetAsync(hist.p, 0, hist.bytes, stream));
 		if (grad_se.p) CU(cudaMemsetAsync(grad_se.p, 0, grad_se.bytes, stream));
 		if (grad_bse.p) CU(cudaMemsetAsync(grad_bse.p, 0, grad_bse.bytes, stream));
+		if (wsign_se.p) CU(cudaMemsetAsync(wsign_se.p, 0, wsign_se.bytes, stream));
+		if (wsign_bse.p) CU(cudaMemsetAsync(wsign_bse.p, 0, wsign_bse.bytes, stream));
 		CU(cudaStreamSynchronize(stream));
 		iteration = 0;
 		kernel_ms = 0;
@@ -653,7 +655,16 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 				T.grad_se = s->grad_se.as<double>();
 				T.grad_bse = s->grad_bse.as<double>();
 			}
+			// signed tallies of the work-function signs (forward and replay
+			// alike) for the work-function derivative of a shifted replay
+			s->wsign_se.alloc(np * 2 * sizeof(int32_t));
+			s->wsign_bse.alloc(np * 2 * sizeof(int32_t));
+			T.wsign_se = s->wsign_se.as<int32_t>();
+			T.wsign_bse = s->wsign_bse.as<int32_t>();
 		}
+		require(params->adjoint_w_step >= 0.0f && params->adjoint_w_step <= 1.0f,
+			"adjoint_w_step must be in [0, 1] eV");
+		sp.wstep = adj ? params->adjoint_w_step : 0.0f;
 		T.n_bins = params->hist_bins > 0 ? params->hist_bins : 200;
 		T.hist_emax = params->hist_emax > 0 ? params->hist_emax : 1000.0f;
 		s->hist.alloc((size_t)T.n_bins * sizeof(uint32_t));
@@ -855,15 +866,44 @@ nbl_status nbl_sim_get_theta(nbl_sim* s, float* theta, int32_t n)
 	});
 }
 
-nbl_status nbl_sim_gradients(nbl_sim* s, double* grad_se, double* grad_bse)
+nbl_status nbl_sim_gradients(nbl_sim* s, const nbl_sim* forward, double* grad_se, double* grad_bse)
 {
 	return guard([&] {
 		require(s && grad_se && grad_bse, "null argument");
 		require(s->params.adjoint && s->grad_se.p, "gradients need adjoint = 1 and a tally grid");
+		const float step = s->sp.wstep;
+		if (step > 0.0f) {
+			require(forward != nullptr, "a replay with adjoint_w_step > 0 needs its forward run");
+			require(forward != s && !forward->params.adjoint && forward->wsign_se.p &&
+				forward->sp.tal.nx == s->sp.tal.nx && forward->sp.tal.ny == s->sp.tal.ny &&
+				forward->sp.key.k0 == s->sp.key.k0 && forward->sp.key.k1 == s->sp.key.k1,
+				"the forward run must be an adjoint = 0 simulation with the same seed and tally grid");
+		}
 		set_device(s->device);
 		CU(cudaMemcpyAsync(grad_se, s->grad_se.p, s->grad_se.bytes, cudaMemcpyDeviceToHost, s->stream));
 		CU(cudaMemcpyAsync(grad_bse, s->grad_bse.p, s->grad_bse.bytes, cudaMemcpyDeviceToHost, s->stream));
 		CU(cudaStreamSynchronize(s->stream));
+		if (step > 0.0f) {
+			// d(count)/dW_m = (sum of r_m over the shifted replay's detections
+			// - the same sum over the forward run's) / step
+			const size_t np = (size_t)s->sp.tal.nx * s->sp.tal.ny;
+			std::vector<int32_t> a(np * 2), f(np * 2);
+			for (int which = 0; which < 2; ++which) {
+				const DevBuf& sa = which ? s->wsign_bse : s->wsign_se;
+				const DevBuf& sf = which ? forward->wsign_bse : forward->wsign_se;
+				CU(cudaMemcpyAsync(a.data(), sa.p, np * 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+				CU(cudaStreamSynchronize(s->stream));
+				set_device(forward->device);
+				CU(cudaMemcpyAsync(f.data(), sf.p, np * 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, forward->stream));
+				CU(cudaStreamSynchronize(forward->stream));
+				set_device(s->device);
+				double* g = which ? grad_bse : grad_se;
+				for (size_t i = 0; i < np; ++i) {
+					g[i * 6 + 2] = (double)(a[2 * i] - f[2 * i]) / step;
+					g[i * 6 + 5] = (double)(a[2 * i + 1] - f[2 * i + 1]) / step;
+				}
+			}
+		}
 	});
 }
 

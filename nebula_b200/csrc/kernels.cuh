@@ -42,6 +42,8 @@ struct Tallies {
 	uint32_t* hist;          // energy histogram [n_bins]
 	double* grad_se;         // adjoint: per pixel d(SE count)/d theta [n_pix][6] (null: off)
 	double* grad_bse;
+	int32_t* wsign_se;       // per pixel sum over detected SE of the primary's work-function
+	int32_t* wsign_bse;      //   signs r_m = +-1, m = 0, 1 [n_pix][2] (null: off)
 	int32_t nx, ny;          // pixel grid
 	int32_t n_bins;
 	float hist_emax;
@@ -71,7 +73,18 @@ struct StepParams {
 	int32_t adjoint;          // accumulate score functions
 	uint32_t refill_below;    // refill primaries only while fewer electrons are in flight
 	uint32_t phys;            // physics selection (PH_* bits)
+	float wstep;              // adjoint replay: work functions shifted by wstep * r_m(primary) (0: off)
 };
+
+// Work-function sign of a primary for material m (0 or 1): +1 or -1 from a
+// hash of the primary's tag and the run's key, the same in every run with
+// that seed.
+__device__ __forceinline__ float wsign(const PhiloxKey& key, uint32_t tag, int m)
+{
+	uint32_t h = tag * 0x9E3779B1u ^ key.k0 ^ (key.k1 * 0x85EBCA77u);
+	h ^= h >> 16; h *= 0x7FEB352Du; h ^= h >> 15; h *= 0x846CA68Bu; h ^= h >> 16;
+	return ((h >> m) & 1u) ? 1.0f : -1.0f;
+}
 
 // One job of a batched run: its geometry, its primaries (a contiguous range
 // of the batch's primary array) and its random-number key.

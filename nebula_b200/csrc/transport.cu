@@ -200,7 +200,7 @@ struct RunView {
 // (drivers/cpu/cpu_driver.inl:74-130, drivers/gpu/gpu_driver.inl:403-480).
 template<bool ADJ>
 __device__ __forceinline__ int free_flight(const StepParams& P, const RunView& rv, Electron& p, int mat, int& last_tri,
-	uint32_t& event, uint32_t stream_tag, uint64_t lineage, float* sc, LocalCounters& lc)
+	uint32_t& event, uint32_t stream_tag, uint64_t lineage, float* sc, LocalCounters& lc, const float* dbar = nullptr)
 {
 	const DevGeometry& G = *rv.geom;
 	for (int hop = 0; hop < 4; ++hop) {
@@ -216,7 +216,8 @@ __device__ __forceinline__ int free_flight(const StepParams& P, const RunView& r
 		const DevMaterial* m = nullptr;
 		if (mat >= 0) {
 			m = P.mats + mat;
-			if (p.E < fa(m->barrier, P.energy_threshold))
+			const float barrier = (ADJ && dbar && mat < 2) ? fa(m->barrier, dbar[mat]) : m->barrier;
+			if (p.E < fa(barrier, P.energy_threshold))
 				return -1;
 			PhiloxStream r;
 			r.init(rv.key, event, 0u, stream_tag, lineage);
@@ -400,6 +401,18 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			rv.key = P.key;
 		}
 
+		// adjoint replay with wstep > 0: this primary's cascade runs with the
+		// work functions shifted by wstep * r_m (the same random numbers as the
+		// forward run otherwise); the work-function derivative is then the
+		// difference of the signed tallies of the two runs, and the
+		// transmission score is not accumulated
+		float dbar[2] = { 0.0f, 0.0f };
+		const bool wshift = ADJ && P.wstep > 0.0f;
+		if (wshift) {
+			dbar[0] = fm(P.wstep, wsign(rv.key, stream_tag, 0));
+			dbar[1] = fm(P.wstep, wsign(rv.key, stream_tag, 1));
+		}
+
 		// interaction that ended the previous flight
 		int status = (kind >= 0) ? ST_RUNNING : ST_TERMINATED;
 		bool spawn = false;
@@ -411,11 +424,13 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			const DevTriangle T = load_tri(rv.geom->tris, last_tri);
 			if (ADJ) {
 				BoundaryScore bs = { 0.0f, 0.0f, -1, -1 };
-				status = boundary_event(T, P.mats, p, mat, r, &bs, P.phys);
+				status = boundary_event(T, P.mats, p, mat, r, &bs, P.phys, wshift ? dbar : nullptr);
 				// the work function enters through barrier = fermi + W of the
 				// materials on either side of the crossing
-				if (bs.mat_in >= 0 && bs.mat_in < 2) sc[3 * bs.mat_in + 2] += bs.d_in;
-				if (bs.mat_out >= 0 && bs.mat_out < 2) sc[3 * bs.mat_out + 2] += bs.d_out;
+				if (!wshift) {
+					if (bs.mat_in >= 0 && bs.mat_in < 2) sc[3 * bs.mat_in + 2] += bs.d_in;
+					if (bs.mat_out >= 0 && bs.mat_out < 2) sc[3 * bs.mat_out + 2] += bs.d_out;
+				}
 			} else {
 				status = boundary_event(T, P.mats, p, mat, r, nullptr, P.phys);
 			}
@@ -449,7 +464,13 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 						double* g = (p.E < 50.0f ? T.grad_se : T.grad_bse) + pix * 6;
 #pragma unroll
 						for (int k = 0; k < 6; ++k)
-							atomicAdd(g + k, (double)sc[k]);
+							if (k % 3 != 2 || !wshift)
+								atomicAdd(g + k, (double)sc[k]);
+					}
+					if (T.wsign_se) {
+						int32_t* w = (p.E < 50.0f ? T.wsign_se : T.wsign_bse) + pix * 2;
+						atomicAdd(w, (int32_t)wsign(rv.key, stream_tag, 0));
+						atomicAdd(w + 1, (int32_t)wsign(rv.key, stream_tag, 1));
 					}
 				}
 			}
@@ -513,7 +534,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		// next free flight
 		int qtype = -1;
 		if (status == ST_RUNNING)
-			qtype = free_flight<ADJ>(P, rv, p, mat, last_tri, event, stream_tag, lineage, sc, lc);
+			qtype = free_flight<ADJ>(P, rv, p, mat, last_tri, event, stream_tag, lineage, sc, lc,
+				wshift ? dbar : nullptr);
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
 			lc.add(CNT_TERMINATED);
 #pragma unroll

@@ -13,10 +13,15 @@ elastic IMFP scale and work function, for materials 0 and 1):
   sums of the score functions of every detected SE; the vector-Jacobian
   product is contracted on the host in float64.
 
-The gradients are the score-function estimator of the C ABI
-(``nbl_sim_gradients``): unbiased for the mean-free-path scales; for the work
-function they include the transmission probability's score and not the
-deterministic energy shift and refraction at a crossing.
+The gradients are those of the C ABI (``nbl_sim_gradients``): score-function
+estimates for the mean-free-path scales; for the work functions, with
+``w_step > 0`` (the default, 0.05 eV), the signed-tally difference of a
+replay whose primaries run with the work functions shifted by
+``w_step * (+-1)``, which carries the deterministic effects of a crossing
+(energy shift, refraction) as well as the transmission probability; with
+``w_step = 0`` the transmission probability's score alone.  With
+``w_step > 0`` the backward pass uses the forward pass's signed tallies, so
+it must follow a forward pass at the same theta (as autograd does).
 """
 from __future__ import annotations
 
@@ -27,7 +32,8 @@ from .api import Simulation
 
 
 class ScanProblem:
-    def __init__(self, geometry, materials, primaries, tally, seed=1, capacity=1 << 21, device=0):
+    def __init__(self, geometry, materials, primaries, tally, seed=1, capacity=1 << 21, device=0, w_step=0.05,
+                 physics=None):
         self.primaries = primaries
         self.tally = tuple(tally)
         nx, ny = self.tally
@@ -35,9 +41,12 @@ class ScanProblem:
         ok = (primaries["px"] >= 0) & (primaries["px"] < nx) & (primaries["py"] >= 0) & (primaries["py"] < ny)
         np.add.at(counts, (primaries["py"][ok], primaries["px"][ok]), 1.0)
         self.per_pixel = counts
-        self.forward_sim = Simulation(geometry, materials, capacity=capacity, seed=seed, tally=tally, device=device)
+        self.w_step = float(w_step)
+        self._forward_theta = None
+        self.forward_sim = Simulation(geometry, materials, capacity=capacity, seed=seed, tally=tally, device=device,
+                                      physics=physics)
         self.adjoint_sim = Simulation(geometry, materials, capacity=capacity, seed=seed, tally=tally, device=device,
-                                      adjoint=True)
+                                      adjoint=True, adjoint_w_step=self.w_step, physics=physics)
 
     def theta0(self):
         return torch.tensor(self.forward_sim.get_theta(), dtype=torch.float64)
@@ -51,14 +60,20 @@ class ScanProblem:
 
     def forward(self, theta):
         self._run(self.forward_sim, theta)
+        self._forward_theta = np.asarray(theta, np.float32).copy()
         se, bse, _ = self.forward_sim.tallies()
         with np.errstate(invalid="ignore", divide="ignore"):
             return np.where(self.per_pixel > 0, se / self.per_pixel, 0.0)
 
     def jacobian(self, theta):
-        """d(SE yield of each pixel)/d theta, shape (ny, nx, 6)."""
+        """d(SE yield of each pixel)/d theta, shape (ny, nx, 6).  With a
+        work-function step, the forward run at the same theta is reused (run
+        here if the last forward pass was at another theta)."""
+        th = np.asarray(theta, np.float32)
+        if self.w_step > 0 and (self._forward_theta is None or not np.array_equal(self._forward_theta, th)):
+            self.forward(th)
         self._run(self.adjoint_sim, theta)
-        gs, _ = self.adjoint_sim.gradients()
+        gs, _ = self.adjoint_sim.gradients(self.forward_sim if self.w_step > 0 else None)
         with np.errstate(invalid="ignore", divide="ignore"):
             return np.where(self.per_pixel[..., None] > 0, gs / self.per_pixel[..., None], 0.0)
 
