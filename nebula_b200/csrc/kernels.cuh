@@ -35,6 +35,7 @@ constexpr int SLOT_TICKETS = 5;
 constexpr int SLOT_SPILL_HEAD = 6;
 constexpr int SLOT_SPILL_TAIL = 7;
 constexpr int SLOT_SPILL_PUSHED = 8;
+constexpr int SLOT_WORK = 9;          // items handed out so far in the iteration that reads the slot
 
 struct Tallies {
 	uint32_t* se_img;        // per pixel counts of detected E < 50 eV (null: off)

@@ -335,10 +335,15 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 	const Queue* qout = P.q[(it + 1u) & 1u];
 
 	const uint32_t lane = threadIdx.x & 31u;
-	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+	// Warps take 32 items at a time from a counter in the read slot (zeroed
+	// two iterations ago, untouched since), so the iteration ends when the
+	// work does rather than when the slowest warp's fixed share does.
+	uint32_t* const work = P.ctrl + rs * SLOT_WORDS + SLOT_WORK;
+	uint32_t base = 0u;
+	if (lane == 0u) base = atomicAdd(work, 32u);
+	base = __shfl_sync(0xFFFFFFFFu, base, 0);
 
-	for (uint32_t base = warp * 32u; base < total; base += n_warps * 32u) {
+	for (; base < total; ) {
 		const uint32_t item = base + lane;
 		int kind = -1;
 		uint32_t qi = 0;
@@ -554,6 +559,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 				}
 			}
 		}
+		if (lane == 0u) base = atomicAdd(work, 32u);
+		base = __shfl_sync(0xFFFFFFFFu, base, 0);
 	}
 	return true;
 }
