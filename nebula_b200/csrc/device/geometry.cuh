@@ -100,29 +100,34 @@ __device__ __forceinline__ int propagate(const DevGeometry& g, float sx, float s
 	uint64_t location = 1;
 	int steps = 0;
 	do {
+		// Cell centre update of the reference, c += (aw * h) * (bit - 0.5)
+		// with aw = 2^-level: both products are exact (power-of-two
+		// scalings of h, far from underflow), so the offset is carried as
+		// +-h 2^-(level+1), halved per level, and only the addition rounds.
 		float ax = g.cx, ay = g.cy, az = g.cz, aw = 1.0f;
+		float ox = fm(g.hx, 0.5f), oy = fm(g.hy, 0.5f), oz = fm(g.hz, 0.5f);
 		int index = 0;
 		// descend to the current location code from the root
 		for (int i = 60 - __clzll((long long)location); i >= 0; i -= 3) {
 			const unsigned int octant = (unsigned int)(location >> i) & 7u;
 			index = __ldg(od + index + octant);
-			ax = fa(ax, fm(fm(aw, g.hx), (float)(octant & 1u) - 0.5f));
-			ay = fa(ay, fm(fm(aw, g.hy), (float)((octant & 2u) >> 1) - 0.5f));
-			az = fa(az, fm(fm(aw, g.hz), (float)((octant & 4u) >> 2) - 0.5f));
+			ax = fa(ax, (octant & 1u) ? ox : -ox);
+			ay = fa(ay, (octant & 2u) ? oy : -oy);
+			az = fa(az, (octant & 4u) ? oz : -oz);
 			aw = fm(aw, 0.5f);
+			ox = fm(ox, 0.5f); oy = fm(oy, 0.5f); oz = fm(oz, 0.5f);
 		}
 		// continue to the leaf that contains the current position
 		while (index >= 0) {
-			unsigned int octant = 0;
-			octant ^= (cx > ax) ? 1u : 0u;
-			octant ^= (cy > ay) ? 2u : 0u;
-			octant ^= (cz > az) ? 4u : 0u;
+			const bool bx = cx > ax, by = cy > ay, bz = cz > az;
+			const unsigned int octant = (bx ? 1u : 0u) | (by ? 2u : 0u) | (bz ? 4u : 0u);
 			location = (location << 3) | octant;
 			index = __ldg(od + index + octant);
-			ax = fa(ax, fm(fm(aw, g.hx), (float)(octant & 1u) - 0.5f));
-			ay = fa(ay, fm(fm(aw, g.hy), (float)((octant & 2u) >> 1) - 0.5f));
-			az = fa(az, fm(fm(aw, g.hz), (float)((octant & 4u) >> 2) - 0.5f));
+			ax = fa(ax, bx ? ox : -ox);
+			ay = fa(ay, by ? oy : -oy);
+			az = fa(az, bz ? oz : -oz);
 			aw = fm(aw, 0.5f);
+			ox = fm(ox, 0.5f); oy = fm(oy, 0.5f); oz = fm(oz, 0.5f);
 		}
 		index = -index;
 

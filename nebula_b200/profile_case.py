@@ -26,6 +26,7 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--workload", default="grating", choices=["grating", "slab"])
+    ap.add_argument("--block", type=int, default=0, help="threads per block of the step kernel (0: default)")
     args = ap.parse_args(argv)
 
     import numpy as np
@@ -47,7 +48,8 @@ def main(argv=None):
             nmat.write(p, materials.build_raw_material(sp))
             ms.append(nb.Material.load(p))
         g = nb.Geometry.from_tri_file(tri)
-        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=args.seed, record_capacity=1 << 22)
+        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=args.seed, record_capacity=1 << 22,
+                            block_size=args.block)
         runs = []
         for r in range(args.repeat + 1):
             sim.reset()
