@@ -508,6 +508,17 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		if (spawn) {
 			lc.add(CNT_SPAWNED);
 			se_lineage = child_lineage(lineage, event);
+			// A secondary below its material's escape threshold ends at its
+			// first free flight (energy cut, before any random draw or
+			// event): count that flight and termination here instead of
+			// queueing it.  Counter-based random numbers make this change
+			// nothing for any other electron.
+			const float barrier = (wshift && mat < 2) ? fa(P.mats[mat].barrier, dbar[mat]) : P.mats[mat].barrier;
+			if (se.E < fa(barrier, P.energy_threshold)) {
+				spawn = false;
+				lc.add(CNT_FLIGHTS);
+				lc.add(CNT_TERMINATED);
+			}
 		}
 		const uint32_t ticket = warp_reserve(cw + SLOT_TICKETS, spawn);
 		const bool queued = spawn && ticket < se_budget;
