@@ -343,7 +343,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--capacity", type=int, default=1 << 21)
+    ap.add_argument("--capacity", type=int, default=1 << 22)
     ap.add_argument("--record-capacity", type=int, default=1 << 24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch (batched vs plain) measurement")

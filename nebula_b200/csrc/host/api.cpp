@@ -82,6 +82,8 @@ struct nbl_sim {
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	double kernel_ms = 0;
 	std::vector<nbl_record> host_records;   // records drained from the device during runs
+	uint32_t records_seen = 0;              // device record count at the last graph boundary
+	uint32_t record_growth = 0;             // most records one graph has added
 	uint32_t* pinned_ctrl = nullptr;
 
 	~nbl_sim()
@@ -160,9 +162,18 @@ struct nbl_sim {
 		for (uint64_t k = 0; k < max_graphs; ++k) {
 			launch_graph();
 			read_ctrl(c);
+			// records stay on the device until the buffer could not take two
+			// more graphs' worth (the most one graph has added so far, at
+			// least 1/8 of the buffer); then they are parked on the host
 			const uint32_t ndet = pinned_ctrl[SLOT_WORDS];
-			if (ndet > sp.det_cap / 4)
+			record_growth = std::max(record_growth, ndet >= records_seen ? ndet - records_seen : ndet);
+			const uint64_t reserve = std::max<uint64_t>(2ull * record_growth, sp.det_cap / 8);
+			if ((uint64_t)ndet + reserve > sp.det_cap) {
 				drain_to_host(ndet);
+				records_seen = 0;
+			} else {
+				records_seen = ndet;
+			}
 			const uint64_t active = (uint64_t)c[0] + c[1] + c[2] + c[3] + spill_occupancy(c);
 			const uint64_t left = n_pri - c[SLOT_CURSOR];
 			if (active == 0 && left == 0)
@@ -227,6 +238,7 @@ struct nbl_sim {
 		iteration = 0;
 		kernel_ms = 0;
 		host_records.clear();
+		records_seen = 0;
 	}
 
 	void ensure_primary_capacity(uint64_t need)
@@ -779,6 +791,7 @@ nbl_status nbl_sim_drain_detected(nbl_sim* s, nbl_record* out, int64_t cap, int6
 		}
 		CU(cudaMemsetAsync(s->n_detected.p, 0, sizeof(uint32_t), s->stream));
 		CU(cudaStreamSynchronize(s->stream));
+		s->records_seen = 0;
 		*n = k + m;
 	});
 }
