@@ -336,6 +336,63 @@ def adjoint_vs_forward(args, dev, workdir, nx=64, per_pixel=10_000, fd=True):
     return out
 
 
+# ---------------------------------------------------------------------------- rough lines
+def rough_lines(args, dev, workdir, rows=128):
+    """Large-mesh plain method: the 16-line grating with line-edge roughness
+    (1.2 M triangles, octree depth <= 12, <= 16 triangles per leaf) at 300 eV,
+    200 primaries per pixel over a band of ``rows`` full raster lines of the
+    512 x 512 scan (the throughput per primary of the whole scan; the band
+    keeps the host-side input generation short).  Reports the host octree
+    build time (all host threads) and the device primaries/s."""
+    import torch
+    import nebula_b200 as nb
+    from nebula_b200.synth import geometry, materials, nmat, primaries
+    t0 = time.perf_counter()
+    tri_rows = geometry.rough_grating()
+    t_gen = time.perf_counter() - t0
+    tris = nb.triangles_from_vertices(tri_rows)
+    t0 = time.perf_counter()
+    g = nb.Geometry.from_triangles(tris, max_depth=12, split_count=16)
+    t_build = time.perf_counter() - t0
+    ms = []
+    for sp in (materials.silicon(), materials.pmma()):
+        pth = os.path.join(workdir, "rough_" + sp.name + ".nmat")
+        nmat.write(pth, materials.build_raw_material(sp))
+        ms.append(nb.Material.load(pth))
+    px, py = np.meshgrid(np.arange(512), np.arange(256 - rows // 2, 256 + rows // 2), indexing="xy")
+    pixels = np.stack([px.ravel(), py.ravel()], 1)
+    pri = primaries.raster_scan(512, 512, 200, 0.5, 300.0, 40.0, spot_sigma=1.0, seed=11, pixels=pixels,
+                                pixel_streams=False)
+    n = len(pri)
+    sim = nb.Simulation(g, ms, capacity=1 << 22, seed=31, record_capacity=1 << 24, tally=(512, 512), device=dev)
+    pri_dev = torch.from_numpy(pri.view(np.uint8)).to(f"cuda:{dev}")
+    sim.reset()
+    sim.push_device(pri_dev.data_ptr(), n)
+    sim.run()                                          # warm-up
+    ms_list, flights = [], 0
+    steps = max(1, min(args.steps, 2))
+    for _ in range(steps):
+        sim.reset()
+        sim.push_device(pri_dev.data_ptr(), n)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        sim.run()
+        torch.cuda.synchronize(dev)
+        ms_list.append((time.perf_counter() - t0) * 1e3)
+        flights = sim.counters()["flights"]
+    se, bse, _ = sim.tallies()
+    info = g.info()
+    sim.close()
+    g.close()
+    t = float(np.mean(ms_list)) / 1e3
+    return {"workload": "rough lines: 16 lines, %d triangles, 512 x %d pixels x 200 primaries at 300 eV (%d primaries)"
+                        % (len(tris), rows, n),
+            "value": n / t, "unit": "primaries/s", "seconds": t, "events_per_primary": flights / n,
+            "se_yield": float(se.sum()) / n, "bse_yield": float(bse.sum()) / n,
+            "octree_words": int(info["n_octree"]), "octree_build_seconds": t_build,
+            "octree_build_threads": os.cpu_count(), "mesh_generation_seconds": t_gen}
+
+
 # ---------------------------------------------------------------------------- GPU
 def main():
     ap = argparse.ArgumentParser()
@@ -348,6 +405,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch (batched vs plain) measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint vs forward measurement")
+    ap.add_argument("--no-rough", action="store_true", help="skip the large-mesh (rough lines) measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -467,6 +525,8 @@ def main():
             out["batched"] = batched_vs_plain(args, dev, d)
         if not args.no_adjoint:
             out["adjoint"] = adjoint_vs_forward(args, dev, d)
+        if not args.no_rough:
+            out["rough_lines"] = rough_lines(args, dev, d)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             try:
                 out["cpu_baseline"] = cpu_baseline(w, tri, mats, d)

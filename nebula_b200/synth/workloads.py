@@ -54,10 +54,10 @@ def grating(nx=256, ny=256, per_pixel=100, energy=500.0, pixels=None, seed=7, e_
                     pri, detector_z=50.0, n_pixels=(nx, ny))
 
 
-def rough(nx=512, ny=512, per_pixel=200, energy=300.0, pixels=None, seed=11):
+def rough(nx=512, ny=512, per_pixel=200, energy=300.0, pixels=None, seed=11, pixel_streams=True):
     tris = geometry.rough_grating()
     pri = primaries.raster_scan(nx, ny, per_pixel, 0.5, energy, GRATING_Z0, spot_sigma=1.0,
-                                seed=seed, pixels=pixels)
+                                seed=seed, pixels=pixels, pixel_streams=pixel_streams)
     return Workload("rough", tris, [materials.silicon(), materials.pmma()], pri,
                     detector_z=50.0, n_pixels=(nx, ny))
 

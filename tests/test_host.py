@@ -157,3 +157,23 @@ def test_material_count_checked(inputs):
     with pytest.raises(nb.NblError) as e:
         nb.Simulation(g, [m], capacity=1024)
     assert e.value.status == 1
+
+
+def test_octree_builder_rough_lines_matches_reference(tmp_path):
+    """Line-edge-roughness grating (the large-mesh geometry at reduced
+    length: 4 lines, 40 nm long, ~25 k triangles): the multithreaded top-down
+    builder gives the reference's incremental builder's octree exactly."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        pytest.skip("reference build not present")
+    from nebula_b200.synth import geometry
+    rows = geometry.rough_grating(n_lines=4, line_length=40.0, size=200.0)
+    p = str(tmp_path / "rough.tri")
+    geometry.write_tri(p, rows)
+    rg = O.RefGeometry(p)
+    g = nb.Geometry.from_tri_file(p)
+    od, tr = g.export()
+    assert len(tr) > 10000
+    assert np.array_equal(od, rg.octree_data)
+    assert np.array_equal(tr["r0"], rg.tri11[:, 2:5])
+    assert np.array_equal(tr["e2"], rg.tri11[:, 8:11])
