@@ -185,6 +185,25 @@ typedef struct nbl_physics_opts {
 void nbl_physics_defaults(nbl_physics_opts* o);
 
 /* ------------------------------------------------------------ simulation */
+/* Energy deposits (the reference's energy-deposit driver,
+ * drivers/cpu/energydeposit_cpu_driver.h:44-93 with the record of
+ * cpu_energydep.cpp:197-204): every scatter event (not a boundary crossing)
+ * that changes the kinetic energy deposits the difference at its position. */
+typedef struct nbl_deposit_record {
+	float pos[3];                /* nm, where the event happened */
+	float energy;                /* eV, kinetic energy before the event */
+	float loss;                  /* eV, energy lost in the event */
+	int32_t px, py;              /* pixel of the primary */
+} nbl_deposit_record;
+/* Voxel grid the losses are summed into on the device (FP64, eV per voxel,
+ * layout [n[2]][n[1]][n[0]]); voxel (i, j, k) covers
+ * origin + (i, j, k) * voxel ... origin + (i+1, j+1, k+1) * voxel.  n = 0: off. */
+typedef struct nbl_deposit_grid {
+	float origin[3];
+	float voxel[3];
+	int32_t n[3];
+} nbl_deposit_grid;
+
 typedef struct nbl_params {
 	int32_t device;              /* CUDA device ordinal */
 	uint32_t capacity;           /* refill target: primaries are added while fewer electrons are in
@@ -204,6 +223,8 @@ typedef struct nbl_params {
 	int32_t adjoint;             /* 1: accumulate score functions (see nbl_sim_gradients) */
 	float adjoint_w_step;        /* eV; > 0: work-function derivative by a shifted replay
 	                                (see nbl_sim_gradients); 0: transmission score only */
+	uint32_t deposit_capacity;   /* deposit records buffered on the device; 0: no records */
+	nbl_deposit_grid deposit_grid; /* voxel grid of the losses; n = 0: none */
 } nbl_params;
 void nbl_params_defaults(nbl_params* p);
 
@@ -218,6 +239,9 @@ typedef struct nbl_counters {
 	uint64_t iterations;         /* wavefront iterations launched */
 	uint64_t primaries_total;    /* primaries pushed */
 	uint64_t records_pending;    /* detected records not yet drained */
+	uint64_t deposits;           /* scatter events that deposited energy */
+	uint64_t deposit_overflow;   /* deposit records lost for lack of buffer room */
+	uint64_t deposits_pending;   /* deposit records not yet drained */
 } nbl_counters;
 
 nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
@@ -251,6 +275,12 @@ nbl_status nbl_sim_set_seed(nbl_sim* s, uint64_t seed);
  * each graph launch), milliseconds. */
 nbl_status nbl_sim_kernel_ms(nbl_sim* s, double* ms);
 void nbl_sim_destroy(nbl_sim* s);
+
+/* Deposit records of the run so far (host copies first, in arrival order
+ * within a graph); the returned ones are removed.  Needs deposit_capacity > 0. */
+nbl_status nbl_sim_drain_deposits(nbl_sim* s, nbl_deposit_record* out, int64_t cap, int64_t* n);
+/* The voxel grid (n[0] * n[1] * n[2] doubles, eV). */
+nbl_status nbl_sim_deposit_grid(nbl_sim* s, double* out);
 
 /* ------------------------------------------------------------ adjoint */
 /* Continuous material parameters theta, 3 per material for up to 2 materials:

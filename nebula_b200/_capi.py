@@ -64,13 +64,18 @@ class PhysicsOpts(C.Structure):
     _fields_ = [(n, C.c_int32) for n in PHYSICS_OPTION_NAMES]
 
 
+class DepositGrid(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("voxel", C.c_float * 3), ("n", C.c_int32 * 3)]
+
+
 class Params(C.Structure):
     _fields_ = [("device", C.c_int32), ("capacity", C.c_uint32), ("energy_threshold", C.c_float),
                 ("seed", C.c_uint64), ("block_size", C.c_uint32), ("grid_size", C.c_uint32),
                 ("iterations_per_graph", C.c_uint32), ("record_capacity", C.c_uint32),
                 ("tally_nx", C.c_int32), ("tally_ny", C.c_int32), ("hist_bins", C.c_int32),
                 ("hist_emax", C.c_float), ("max_events", C.c_uint32), ("stream", C.c_void_p),
-                ("physics", PhysicsOpts), ("adjoint", C.c_int32), ("adjoint_w_step", C.c_float)]
+                ("physics", PhysicsOpts), ("adjoint", C.c_int32), ("adjoint_w_step", C.c_float),
+                ("deposit_capacity", C.c_uint32), ("deposit_grid", DepositGrid)]
 
 
 class BatchJob(C.Structure):
@@ -88,7 +93,7 @@ class BatchParams(C.Structure):
 COUNTER_NAMES = ("flights", "boundary", "elastic", "inelastic", "spawned", "detected", "terminated",
                  "primaries_started", "walk_overflow", "nan_state", "queue_overflow",
                  "record_overflow", "event_budget", "spilled", "iterations", "primaries_total",
-                 "records_pending")
+                 "records_pending", "deposits", "deposit_overflow", "deposits_pending")
 
 
 class Counters(C.Structure):
@@ -131,6 +136,8 @@ _DECLS = [
     ("nbl_sim_set_theta", C.c_int, [C.c_void_p, f32p, C.c_int32]),
     ("nbl_sim_get_theta", C.c_int, [C.c_void_p, f32p, C.c_int32]),
     ("nbl_sim_gradients", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("nbl_sim_drain_deposits", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, i64p]),
+    ("nbl_sim_deposit_grid", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_destroy", None, [C.c_void_p]),
     ("nbl_batch_params_defaults", None, [C.POINTER(BatchParams)]),

@@ -15,6 +15,8 @@ from . import _capi
 from ._capi import lib, check
 
 PRI_DTYPE = np.dtype([("pos", "<f4", 3), ("dir", "<f4", 3), ("E", "<f4"), ("px", "<i4"), ("py", "<i4")])
+# nbl_deposit_record: position, energy before the event, energy lost, pixel (28 bytes)
+DEPOSIT_DTYPE = np.dtype([("pos", "<f4", 3), ("E", "<f4"), ("loss", "<f4"), ("px", "<i4"), ("py", "<i4")])
 assert PRI_DTYPE.itemsize == C.sizeof(_capi.Record) == 36
 TRI_DTYPE = np.dtype([("material_in", "<i4"), ("material_out", "<i4"), ("r0", "<f4", 3), ("e1", "<f4", 3),
                       ("e2", "<f4", 3)])
@@ -231,7 +233,7 @@ class Simulation:
     def __init__(self, geometry, materials, capacity=1 << 20, seed=0x78C7E39B, energy_threshold=0.0, device=0,
                  tally=(0, 0), hist_bins=200, hist_emax=1000.0, record_capacity=0, block_size=0, grid_size=0,
                  iterations_per_graph=0, max_events=0, adjoint=False, stream=None, physics=None,
-                 adjoint_w_step=0.0):
+                 adjoint_w_step=0.0, deposit_capacity=0, deposit_grid=None):
         p = _capi.Params()
         lib().nbl_params_defaults(C.byref(p))
         p.physics = physics_options(physics)
@@ -249,6 +251,14 @@ class Simulation:
         p.max_events = max_events
         p.adjoint = int(bool(adjoint))
         p.adjoint_w_step = adjoint_w_step
+        p.deposit_capacity = deposit_capacity
+        self.deposit_grid_shape = None
+        if deposit_grid is not None:
+            origin, voxel, n = deposit_grid
+            p.deposit_grid.origin[:] = [float(v) for v in origin]
+            p.deposit_grid.voxel[:] = [float(v) for v in voxel]
+            p.deposit_grid.n[:] = [int(v) for v in n]
+            self.deposit_grid_shape = (int(n[2]), int(n[1]), int(n[0]))
         p.stream = stream
         self.params = p
         self.tally = tuple(tally)
@@ -348,6 +358,26 @@ class Simulation:
                                       gs.ctypes.data_as(C.POINTER(C.c_double)),
                                       gb.ctypes.data_as(C.POINTER(C.c_double))))
         return gs, gb
+
+    def drain_deposits(self):
+        """Energy-deposit records of the run so far (DEPOSIT_DTYPE), removed
+        from the simulation."""
+        parts = []
+        chunk = 1 << 22
+        while True:
+            out = np.empty(chunk, DEPOSIT_DTYPE)
+            n = C.c_int64()
+            check(lib().nbl_sim_drain_deposits(self._h, out.ctypes.data, chunk, C.byref(n)))
+            parts.append(out[:n.value])
+            if n.value < chunk:
+                break
+        return np.concatenate(parts)
+
+    def deposit_grid(self):
+        """Deposited energy per voxel (eV, float64), shape (nz, ny, nx)."""
+        g = np.zeros(self.deposit_grid_shape, np.float64)
+        check(lib().nbl_sim_deposit_grid(self._h, g.ctypes.data_as(C.POINTER(C.c_double))))
+        return g
 
     def reset(self):
         check(lib().nbl_sim_reset(self._h))

@@ -71,6 +71,9 @@ struct nbl_sim {
 	DevBuf queues[2][N_QUEUES][6];
 	DevBuf spill[6];
 	DevBuf ctrl, counters, detected, n_detected, se_img, bse_img, hist, grad_se, grad_bse, wsign_se, wsign_bse;
+	DevBuf deposits, n_deposits, dep_grid;
+	std::vector<nbl_deposit_record> host_deposits;   // deposit records drained during runs
+	uint32_t deposits_seen = 0, deposit_growth = 0;
 	DevBuf primaries;
 	uint64_t pri_cap = 0, n_pri = 0;
 	StepParams sp{};
@@ -153,6 +156,19 @@ struct nbl_sim {
 		CU(cudaStreamSynchronize(stream));
 	}
 
+	// Move device deposit records to the host store.
+	void drain_deposits_to_host(uint32_t n_dev)
+	{
+		const uint32_t n = std::min(n_dev, sp.dep_cap);
+		if (n == 0) return;
+		const size_t old = host_deposits.size();
+		host_deposits.resize(old + n);
+		CU(cudaMemcpyAsync(host_deposits.data() + old, deposits.p, (size_t)n * sizeof(nbl_deposit_record),
+			cudaMemcpyDeviceToHost, stream));
+		CU(cudaMemsetAsync(n_deposits.p, 0, sizeof(uint32_t), stream));
+		CU(cudaStreamSynchronize(stream));
+	}
+
 	// Run graphs until done (or `max_graphs` graphs); returns electrons still
 	// in flight plus primaries not yet started.
 	int64_t advance(uint64_t max_graphs)
@@ -173,6 +189,20 @@ struct nbl_sim {
 				records_seen = 0;
 			} else {
 				records_seen = ndet;
+			}
+			if (sp.dep) {
+				// deposit records: the same rule
+				uint32_t ndep = 0;
+				CU(cudaMemcpyAsync(&ndep, n_deposits.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+				CU(cudaStreamSynchronize(stream));
+				deposit_growth = std::max(deposit_growth, ndep >= deposits_seen ? ndep - deposits_seen : ndep);
+				const uint64_t dres = std::max<uint64_t>(2ull * deposit_growth, sp.dep_cap / 8);
+				if ((uint64_t)ndep + dres > sp.dep_cap) {
+					drain_deposits_to_host(ndep);
+					deposits_seen = 0;
+				} else {
+					deposits_seen = ndep;
+				}
 			}
 			const uint64_t active = (uint64_t)c[0] + c[1] + c[2] + c[3] + spill_occupancy(c);
 			const uint64_t left = n_pri - c[SLOT_CURSOR];
@@ -211,6 +241,9 @@ struct nbl_sim {
 		unsigned long long cnt[N_COUNTERS];
 		CU(cudaMemcpyAsync(cnt, counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
 		CU(cudaStreamSynchronize(stream));
+		if (cnt[CNT_DEPOSIT_OVERFLOW])
+			throw Error(NBL_ERR_POOL_OVERFLOW, std::to_string(cnt[CNT_DEPOSIT_OVERFLOW]) +
+				" deposit records dropped; raise deposit_capacity");
 		if (cnt[CNT_QUEUE_OVERFLOW] || cnt[CNT_RECORD_OVERFLOW])
 			throw Error(NBL_ERR_POOL_OVERFLOW, "secondary overflow ring or record buffer full (" +
 				std::to_string(cnt[CNT_QUEUE_OVERFLOW]) + " electrons, " + std::to_string(cnt[CNT_RECORD_OVERFLOW]) +
@@ -234,7 +267,11 @@ struct nbl_sim {
 		if (grad_bse.p) CU(cudaMemsetAsync(grad_bse.p, 0, grad_bse.bytes, stream));
 		if (wsign_se.p) CU(cudaMemsetAsync(wsign_se.p, 0, wsign_se.bytes, stream));
 		if (wsign_bse.p) CU(cudaMemsetAsync(wsign_bse.p, 0, wsign_bse.bytes, stream));
+		if (n_deposits.p) CU(cudaMemsetAsync(n_deposits.p, 0, n_deposits.bytes, stream));
+		if (dep_grid.p) CU(cudaMemsetAsync(dep_grid.p, 0, dep_grid.bytes, stream));
 		CU(cudaStreamSynchronize(stream));
+		host_deposits.clear();
+		deposits_seen = 0;
 		iteration = 0;
 		kernel_ms = 0;
 		host_records.clear();
@@ -677,6 +714,30 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		require(params->adjoint_w_step >= 0.0f && params->adjoint_w_step <= 1.0f,
 			"adjoint_w_step must be in [0, 1] eV");
 		sp.wstep = adj ? params->adjoint_w_step : 0.0f;
+		if (params->deposit_capacity) {
+			sp.dep_cap = params->deposit_capacity;
+			s->deposits.alloc((size_t)sp.dep_cap * sizeof(DepositRecord));
+			s->n_deposits.alloc(sizeof(uint32_t));
+			sp.dep = s->deposits.as<DepositRecord>();
+			sp.n_dep = s->n_deposits.as<uint32_t>();
+		}
+		{
+			const nbl_deposit_grid& dg = params->deposit_grid;
+			const int64_t nv = (int64_t)dg.n[0] * dg.n[1] * dg.n[2];
+			if (dg.n[0] || dg.n[1] || dg.n[2]) {
+				require(dg.n[0] > 0 && dg.n[1] > 0 && dg.n[2] > 0 && nv < ((int64_t)1 << 31),
+					"deposit grid dimensions must be positive and below 2^31 voxels in all");
+				for (int k = 0; k < 3; ++k) {
+					require(dg.voxel[k] > 0 && std::isfinite(dg.voxel[k]) && std::isfinite(dg.origin[k]),
+						"deposit grid voxels must be positive and finite");
+					sp.g_org[k] = dg.origin[k];
+					sp.g_inv[k] = 1.0f / dg.voxel[k];
+					sp.gn[k] = dg.n[k];
+				}
+				s->dep_grid.alloc((size_t)nv * sizeof(double));
+				sp.grid = s->dep_grid.as<double>();
+			}
+		}
 		T.n_bins = params->hist_bins > 0 ? params->hist_bins : 200;
 		T.hist_emax = params->hist_emax > 0 ? params->hist_emax : 1000.0f;
 		s->hist.alloc((size_t)T.n_bins * sizeof(uint32_t));
@@ -832,6 +893,45 @@ nbl_status nbl_sim_counters(nbl_sim* s, nbl_counters* out)
 		out->iterations = s->iteration;
 		out->primaries_total = s->n_pri;
 		out->records_pending = s->host_records.size() + std::min(d, s->sp.det_cap);
+		out->deposits = c[CNT_DEPOSITS];
+		out->deposit_overflow = c[CNT_DEPOSIT_OVERFLOW];
+		uint32_t nd = 0;
+		if (s->n_deposits.p) {
+			CU(cudaMemcpyAsync(&nd, s->n_deposits.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+			CU(cudaStreamSynchronize(s->stream));
+		}
+		out->deposits_pending = s->host_deposits.size() + std::min(nd, s->sp.dep_cap);
+	});
+}
+
+nbl_status nbl_sim_drain_deposits(nbl_sim* s, nbl_deposit_record* out, int64_t cap, int64_t* n)
+{
+	return guard([&] {
+		require(s && n && (out || cap == 0) && cap >= 0, "null argument");
+		require(s->sp.dep != nullptr, "the simulation was created without deposit records (deposit_capacity = 0)");
+		set_device(s->device);
+		s->drain_deposits_to_host([&] {
+			uint32_t d = 0;
+			CU(cudaMemcpyAsync(&d, s->n_deposits.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+			CU(cudaStreamSynchronize(s->stream));
+			return d;
+		}());
+		s->deposits_seen = 0;
+		const int64_t k = std::min<int64_t>(cap, (int64_t)s->host_deposits.size());
+		if (k > 0) std::memcpy(out, s->host_deposits.data(), (size_t)k * sizeof(nbl_deposit_record));
+		s->host_deposits.erase(s->host_deposits.begin(), s->host_deposits.begin() + k);
+		*n = k;
+	});
+}
+
+nbl_status nbl_sim_deposit_grid(nbl_sim* s, double* out)
+{
+	return guard([&] {
+		require(s && out, "null argument");
+		require(s->sp.grid != nullptr, "the simulation was created without a deposit grid");
+		set_device(s->device);
+		CU(cudaMemcpyAsync(out, s->dep_grid.p, s->dep_grid.bytes, cudaMemcpyDeviceToHost, s->stream));
+		CU(cudaStreamSynchronize(s->stream));
 	});
 }
 

@@ -23,7 +23,7 @@ struct Queue {
 enum : int {
 	CNT_FLIGHTS = 0, CNT_BOUNDARY, CNT_ELASTIC, CNT_INELASTIC, CNT_SPAWNED, CNT_DETECTED,
 	CNT_TERMINATED, CNT_PRIMARIES, CNT_WALK_OVERFLOW, CNT_NAN, CNT_QUEUE_OVERFLOW,
-	CNT_RECORD_OVERFLOW, CNT_EVENT_BUDGET, CNT_SPILLED, N_COUNTERS
+	CNT_RECORD_OVERFLOW, CNT_EVENT_BUDGET, CNT_SPILLED, CNT_DEPOSITS, CNT_DEPOSIT_OVERFLOW, N_COUNTERS
 };
 
 // Per-iteration control words, three rotating slots of 16 words:
@@ -75,6 +75,13 @@ struct StepParams {
 	uint32_t refill_below;    // refill primaries only while fewer electrons are in flight
 	uint32_t phys;            // physics selection (PH_* bits)
 	float wstep;              // adjoint replay: work functions shifted by wstep * r_m(primary) (0: off)
+	// energy deposits of scatter events (null: off)
+	DepositRecord* dep;       // records [dep_cap]
+	uint32_t* n_dep;
+	uint32_t dep_cap;
+	double* grid;             // eV per voxel [gn[2]][gn[1]][gn[0]]
+	float g_org[3], g_inv[3]; // grid origin, 1 / voxel size
+	int32_t gn[3];
 };
 
 // Work-function sign of a primary for material m (0 or 1): +1 or -1 from a

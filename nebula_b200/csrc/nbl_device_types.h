@@ -86,4 +86,12 @@ struct Record36 {
 };
 static_assert(sizeof(Record36) == 36, "Record36 must be 36 bytes");
 
+// 28-byte energy-deposit record of a scatter event (cpu_energydep.cpp:197-204):
+// position, kinetic energy before the event, energy lost, pixel.
+struct DepositRecord {
+	float x, y, z, E, dE;
+	int32_t px, py;
+};
+static_assert(sizeof(DepositRecord) == 28, "DepositRecord must be 28 bytes");
+
 }  // namespace nbl

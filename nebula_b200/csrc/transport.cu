@@ -285,8 +285,55 @@ __device__ __forceinline__ uint32_t job_of(const BatchParams& B, uint32_t g)
 // BATCH: electrons carry their job in the tag's top 8 bits (the low 24 bits
 // are the primary's index within its job, which keys its random numbers, as
 // in a run of that job alone); geometry, key and yield tallies are per job.
+// Energy deposit of one scatter event (energydeposit_cpu_driver.h:44-93):
+// a 28-byte record and / or the loss added to its voxel.  Called by the whole
+// warp together; `s_loss` is the warp's 32 floats of shared memory.  Lanes
+// that hit the same voxel are summed first (one double atomic per voxel).
+__device__ __forceinline__ void deposit(const StepParams& P, bool scat, const Electron& p, float e_before,
+	const Record36* pr, float* s_loss, LocalCounters& lc)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	const float loss = scat ? fs(e_before, p.E) : 0.0f;
+	if (P.dep) {
+		const uint32_t slot = warp_reserve(P.n_dep, scat);
+		if (scat) {
+			if (slot < P.dep_cap) {
+				DepositRecord r;
+				r.x = p.pos.x; r.y = p.pos.y; r.z = p.pos.z; r.E = e_before; r.dE = loss;
+				r.px = pr->px; r.py = pr->py;
+				P.dep[slot] = r;
+			} else {
+				lc.add(CNT_DEPOSIT_OVERFLOW);
+			}
+		}
+	}
+	if (P.grid) {
+		int v = -1;
+		if (scat) {
+			const int i = __float2int_rd(fm(fs(p.pos.x, P.g_org[0]), P.g_inv[0]));
+			const int j = __float2int_rd(fm(fs(p.pos.y, P.g_org[1]), P.g_inv[1]));
+			const int k = __float2int_rd(fm(fs(p.pos.z, P.g_org[2]), P.g_inv[2]));
+			if (i >= 0 && j >= 0 && k >= 0 && i < P.gn[0] && j < P.gn[1] && k < P.gn[2])
+				v = (k * P.gn[1] + j) * P.gn[0] + i;
+		}
+		const unsigned peers = __match_any_sync(0xFFFFFFFFu, v);
+		s_loss[lane] = loss;
+		__syncwarp();
+		if (v >= 0 && (int)lane == __ffs(peers) - 1) {
+			double sum = 0.0;
+			for (unsigned m = peers; m; m &= m - 1u)
+				sum += (double)s_loss[__ffs(m) - 1];
+			atomicAdd(P.grid + v, sum);
+		}
+		__syncwarp();
+	}
+	if (scat)
+		lc.add(CNT_DEPOSITS);
+}
+
 template<bool ADJ, bool BATCH>
-__device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc)
+__device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc,
+	float* s_lane = nullptr)
 {
 	const uint32_t rs = it % 3u, ws = (it + 1u) % 3u, zs = (it + 2u) % 3u;
 	const uint32_t* cr = P.ctrl + rs * SLOT_WORDS;
@@ -389,6 +436,7 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			}
 			lc.add(CNT_PRIMARIES);
 		}
+		const float e_before = p.E;
 		// run context: job geometry / key, the primary's record, the tag that
 		// keys the random numbers
 		RunView rv;
@@ -452,6 +500,11 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			r.init(rv.key, event, 1u, stream_tag, lineage);
 			spawn = inelastic_event(P.mats[mat], p, se, r, P.phys);
 		}
+
+		// energy deposit of a scatter event that changed the energy
+		if (!BATCH && (P.dep || P.grid))
+			deposit(P, (kind == EV_ELASTIC || kind == EV_INELASTIC) && p.E != e_before, p, e_before,
+				P.primaries + rec_index, s_lane + (threadIdx.x & ~31u), lc);
 
 		// detection output: record + tallies
 		if (status == ST_DETECTED) {
@@ -591,12 +644,13 @@ template<bool ADJ>
 __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
+	__shared__ float s_lane[256];
 	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
 		s_counters[k] = 0u;
 	__syncthreads();
 	LocalCounters lc{ s_counters };
 	const BatchParams none{};
-	step_iteration<ADJ, false>(P, none, it, lc);
+	step_iteration<ADJ, false>(P, none, it, lc, s_lane);
 	flush_counters(P, s_counters);
 }
 

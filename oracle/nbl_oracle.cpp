@@ -688,6 +688,10 @@ struct driver {
 	}
 	bool active(size_t idx) const { return mgr.p[idx].status != TERMINATED && mgr.p[idx].status != DETECTED; }
 
+	// energy-deposit driver (energydeposit_cpu_driver.h:44-93): called for a
+	// scatter event (not a crossing) that changed the kinetic energy
+	std::function<void(const pstate& before, const pstate& after)> on_deposit;
+
 	// push one primary, simulate_to_end (simple_cpu_driver.h:53-65), flush
 	template<typename F>
 	void run_one(const float* f, int64_t& events, F emit)
@@ -697,7 +701,17 @@ struct driver {
 		mgr.p.push_back({ NO_EVENT, 0, VACUUM, { f[0], f[1], f[2] }, { f[3], f[4], f[5] }, f[6], -1 });
 		for (size_t i = 0; i < mgr.p.size(); ++i)
 			while (active(i)) {
-				init(i); intersect(i); scatter(i); ++events;
+				init(i);
+				if (on_deposit) {
+					const bool track = mgr.p[i].status == SCATTER_EVENT;
+					const pstate before = mgr.p[i];
+					intersect(i); scatter(i); ++events;
+					const pstate after = mgr.p[i];
+					if (track && before.E != after.E)
+						on_deposit(before, after);
+				} else {
+					intersect(i); scatter(i); ++events;
+				}
 				if (std::getenv("NBL_TRACE")) {
 					const pstate& q = mgr.p[i];
 					std::fprintf(stderr, "O %zu %d %d %.9g %.9g %.9g %.9g %.9g %.9g %.9g\n", i, (int)q.status, q.material,
@@ -1047,6 +1061,57 @@ extern "C" int64_t orc_simulate(const orc_geometry* g, const orc_material* mats,
 	*n_total = total;
 	*n_events = events;
 	return written;
+}
+
+extern "C" int64_t orc_simulate_deposits(const orc_geometry* g, const orc_material* mats, int n_mat,
+	const void* pri, int64_t n_pri, uint32_t seed, float energy_threshold, int n_threads,
+	void* out, int64_t max_out, int64_t* n_total, int64_t* n_events)
+{
+	(void)n_mat;
+	if (n_threads < 1) n_threads = 1;
+	std::vector<uint32_t> seeds;
+	if (n_threads == 1) {
+		seeds.push_back(seed);
+	} else {
+		orc_rng* master = orc_rng_mt(seed);
+		for (int t = 0; t < n_threads; ++t) seeds.push_back(mt_next(master));
+		orc_rng_free(master);
+	}
+	std::atomic<int64_t> cursor(0), written(0), events(0);
+	const char* in = static_cast<const char*>(pri);
+	char* o = static_cast<char*>(out);
+	std::vector<std::thread> th;
+	for (int t = 0; t < n_threads; ++t) {
+		th.emplace_back([&, t]() {
+			orc_rng* rng = orc_rng_mt(seeds[t]);
+			driver d{ g, mats, energy_threshold, rng, {} };
+			int64_t ev = 0;
+			int32_t px[2] = { 0, 0 };
+			// record of cpu_energydep.cpp:197-204: after.pos, before.E, before.E - after.E, pixel
+			d.on_deposit = [&](const pstate& before, const pstate& after) {
+				const int64_t w = written++;
+				if (w < max_out) {
+					const float r[5] = { after.pos.x, after.pos.y, after.pos.z, before.E, before.E - after.E };
+					std::memcpy(o + 28 * w, r, 20);
+					std::memcpy(o + 28 * w + 20, px, 8);
+				}
+			};
+			for (;;) {
+				const int64_t i = cursor++;
+				if (i >= n_pri) break;
+				float f[7];
+				std::memcpy(f, in + 36 * i, 28);
+				std::memcpy(px, in + 36 * i + 28, 8);
+				d.run_one(f, ev, [](const pstate&) {});
+			}
+			events += ev;
+			orc_rng_free(rng);
+		});
+	}
+	for (auto& x : th) x.join();
+	*n_total = written;
+	*n_events = events;
+	return std::min<int64_t>(written, max_out);
 }
 
 extern "C" int64_t orc_simulate_mt(const orc_geometry* g, const orc_material* mats, int n_mat,

@@ -100,6 +100,16 @@ int64_t orc_simulate_mt(const orc_geometry* g, const orc_material* mats, int n_m
 	const void* pri, int64_t n_pri, uint32_t seed, float energy_threshold, int n_threads,
 	void* out, int64_t max_out, int64_t* n_total, int64_t* n_events);
 
+/* The energy-deposit driver loop (energydeposit_cpu_driver.h:44-93) over
+ * `n_threads` threads (1: the primaries in order with mt19937(seed), as the
+ * reference run on one thread; more: per-thread seeds as orc_simulate_mt).
+ * Writes 28-byte deposit records (after.pos, before.E, before.E - after.E,
+ * pixel) for every scatter event that changed the energy; returns records
+ * written, *n_total all of them. */
+int64_t orc_simulate_deposits(const orc_geometry* g, const orc_material* mats, int n_mat,
+	const void* pri, int64_t n_pri, uint32_t seed, float energy_threshold, int n_threads,
+	void* out, int64_t max_out, int64_t* n_total, int64_t* n_events);
+
 #ifdef __cplusplus
 }
 #endif

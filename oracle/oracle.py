@@ -48,6 +48,7 @@ def physics_bits(physics=None):
     return b
 PRI_DTYPE = np.dtype([("pos", "<f4", 3), ("dir", "<f4", 3), ("E", "<f4"),
                       ("px", "<i4"), ("py", "<i4")])
+DEPOSIT_DTYPE = np.dtype([("pos", "<f4", 3), ("E", "<f4"), ("loss", "<f4"), ("px", "<i4"), ("py", "<i4")])
 
 f32p = C.POINTER(C.c_float)
 i32p = C.POINTER(C.c_int32)
@@ -113,6 +114,10 @@ def lib():
             fn.restype = C.c_int64
             fn.argtypes = [C.POINTER(OrcGeometry), C.POINTER(OrcMaterial), C.c_int, C.c_void_p,
                            C.c_int64, C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p, i64p]
+        L.orc_simulate_deposits.restype = C.c_int64
+        L.orc_simulate_deposits.argtypes = [C.POINTER(OrcGeometry), C.POINTER(OrcMaterial), C.c_int,
+                                            C.c_void_p, C.c_int64, C.c_uint32, C.c_float, C.c_int,
+                                            C.c_void_p, C.c_int64, i64p, i64p]
         L.orc_set_physics.argtypes = [C.c_uint32]
         L.orc_get_physics.restype = C.c_uint32
         L.orc_simulate_mt.restype = C.c_int64
@@ -272,6 +277,9 @@ def ref():
         L.ref_event.restype = C.c_int
         L.ref_event.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_uint32, C.c_int, C.c_int32,
                                 C.c_uint32, f32p, i32p, f32p, C.c_int, i32p]
+        L.ref_simulate_deposits.restype = C.c_int64
+        L.ref_simulate_deposits.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_void_p, C.c_int64,
+                                            C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p]
         L.ref_simulate.restype = C.c_int64
         L.ref_simulate.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_uint32, C.c_void_p,
                                    C.c_int64, C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p, i64p]
@@ -375,3 +383,33 @@ def ref_simulate(geom, mats, pri, seed, energy_threshold=0.0, max_records=None, 
     if n < 0:
         raise RuntimeError(ref().ref_last_error().decode())
     return out[:n], tot.value, ev.value
+
+
+def simulate_deposits(geom, mats, pri, seed, energy_threshold=0.0, threads=1, max_records=None, phys=PHYS_DEFAULT):
+    """The oracle's energy-deposit driver loop; returns (deposits, n_events)."""
+    pri = np.ascontiguousarray(pri, PRI_DTYPE)
+    cap = max_records if max_records is not None else max(1024, 600 * len(pri))
+    out = np.zeros(cap, DEPOSIT_DTYPE)
+    tot = C.c_int64(0)
+    ev = C.c_int64(0)
+    arr = materials_array(mats)
+    with _physics(phys):
+        n = lib().orc_simulate_deposits(C.byref(geom.s), arr, len(mats), pri.ctypes.data, len(pri), seed,
+                                        energy_threshold, threads, out.ctypes.data, cap, C.byref(tot), C.byref(ev))
+    if tot.value > cap:
+        raise RuntimeError("deposit buffer too small")
+    return out[:n], ev.value
+
+
+def ref_simulate_deposits(geom, mats, pri, seed, energy_threshold=0.0, max_records=None):
+    """The reference's energy-deposit driver (default physics, one thread)."""
+    pri = np.ascontiguousarray(pri, PRI_DTYPE)
+    cap = max_records if max_records is not None else max(1024, 600 * len(pri))
+    out = np.zeros(cap, DEPOSIT_DTYPE)
+    tot = C.c_int64(0)
+    hs = (C.c_void_p * len(mats))(*[x.h for x in mats])
+    n = ref().ref_simulate_deposits(geom.h, hs, len(mats), pri.ctypes.data, len(pri), seed, energy_threshold,
+                                    out.ctypes.data, cap, C.byref(tot))
+    if tot.value > cap:
+        raise RuntimeError("deposit buffer too small")
+    return out[:n]

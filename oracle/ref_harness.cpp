@@ -59,6 +59,7 @@
 #include "core/material.h"
 #include "io/load_tri_file.h"
 #include "drivers/cpu/simple_cpu_driver.h"
+#include "drivers/cpu/energydeposit_cpu_driver.h"
 #include "geometry/octree.h"
 #undef private
 #undef protected
@@ -544,6 +545,49 @@ int64_t ref_simulate(void* gh, void** mats, int n_mat, uint32_t phys, const void
 		g_err = "physics preset not compiled in the harness";
 		return -1;
 	}
+}
+
+/* The reference's energy-deposit driver (energydeposit_cpu_driver.h:44-93),
+ * default physics, one driver seeded with `seed`, primaries one at a time as
+ * cpu_energydep.cpp:170-205 does on one thread; writes its 28-byte deposit
+ * records (after.pos, before.kin_energy, before - after, pixel).  Returns
+ * records written; *n_total all of them. */
+int64_t ref_simulate_deposits(void* gh, void** mats, int n_mat, const void* pri_records, int64_t n_pri,
+	uint32_t seed, float energy_threshold, void* out_records, int64_t max_records, int64_t* n_total)
+{
+	using dep_driver_t = nbl::drivers::energydeposit_cpu_driver<scatter_physics<false>, intersect_t, geometry_t>;
+	auto* g = static_cast<ref_geometry*>(gh);
+	std::vector<material_t> materials;
+	for (int i = 0; i < n_mat; ++i)
+		materials.emplace_back(static_cast<ref_material*>(mats[i])->file);
+	intersect_t inter;
+	dep_driver_t d(g->oct, inter, materials, energy_threshold, seed);
+	int64_t written = 0, total = 0;
+	const char* in = static_cast<const char*>(pri_records);
+	char* out = static_cast<char*>(out_records);
+	for (int64_t i = 0; i < n_pri; ++i)
+	{
+		float f[7]; int32_t px[2];
+		std::memcpy(f, in + 36 * i, 28);
+		std::memcpy(px, in + 36 * i + 28, 8);
+		particle p{ { f[0], f[1], f[2] }, { f[3], f[4], f[5] }, f[6] };
+		uint32_t tag = 0;
+		d.push(&p, &tag, 1);
+		d.simulate_to_end([&](particle const & before, particle const & after, uint32_t) {
+			if (written < max_records)
+			{
+				const float r[5] = { after.pos.x, after.pos.y, after.pos.z,
+					before.kin_energy, before.kin_energy - after.kin_energy };
+				std::memcpy(out + 28 * written, r, 20);
+				std::memcpy(out + 28 * written + 20, px, 8);
+				++written;
+			}
+			++total;
+		});
+		d.flush_detected([](particle, uint32_t) {});
+	}
+	*n_total = total;
+	return written;
 }
 
 } // extern "C"

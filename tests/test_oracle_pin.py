@@ -102,3 +102,21 @@ def test_oracle_grating_records_bit_exact_vs_reference(inputs):
     b = O.simulate(og, oms, w.primaries, 77)
     assert a[2] == b[2] and a[1] == b[1]
     assert a[0].tobytes() == b[0].tobytes()
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_oracle_deposits_bit_exact_vs_reference(inputs):
+    """Energy-deposit driver (energydeposit_cpu_driver.h:44-93): the oracle's
+    deposit records equal the reference's byte for byte (grating, 2 pixels x
+    30 primaries, one thread)."""
+    rg = O.RefGeometry(inputs["grating.tri"])
+    og = rg.oracle_geometry()
+    rms = [O.RefMaterial(inputs["si.nmat"]), O.RefMaterial(inputs["pmma.nmat"])]
+    oms = [O.Material(inputs["si.nmat"]), O.Material(inputs["pmma.nmat"])]
+    from nebula_b200.synth import workloads
+    w = workloads.grating(pixels=[(100, 120), (140, 30)], per_pixel=30)
+    a = O.ref_simulate_deposits(rg, rms, w.primaries, 41)
+    b, ev = O.simulate_deposits(og, oms, w.primaries, 41)
+    assert len(a) > 1000
+    assert a.tobytes() == b.tobytes()
+    assert np.all(a["loss"] != 0)
