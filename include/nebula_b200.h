@@ -204,6 +204,14 @@ typedef struct nbl_deposit_grid {
 	int32_t n[3];
 } nbl_deposit_grid;
 
+/* Detector acceptance of the per-pixel SE / BSE images (the records are not
+ * filtered): a detected electron counts when the cosine of the angle between
+ * its direction and +z lies in [cos_min, cos_max].  enabled = 0: all count. */
+typedef struct nbl_image_filter {
+	int32_t enabled;
+	float cos_min, cos_max;
+} nbl_image_filter;
+
 typedef struct nbl_params {
 	int32_t device;              /* CUDA device ordinal */
 	uint32_t capacity;           /* refill target: primaries are added while fewer electrons are in
@@ -225,6 +233,7 @@ typedef struct nbl_params {
 	                                (see nbl_sim_gradients); 0: transmission score only */
 	uint32_t deposit_capacity;   /* deposit records buffered on the device; 0: no records */
 	nbl_deposit_grid deposit_grid; /* voxel grid of the losses; n = 0: none */
+	nbl_image_filter image_filter; /* detector acceptance of the per-pixel images */
 } nbl_params;
 void nbl_params_defaults(nbl_params* p);
 

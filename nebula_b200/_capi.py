@@ -68,6 +68,10 @@ class DepositGrid(C.Structure):
     _fields_ = [("origin", C.c_float * 3), ("voxel", C.c_float * 3), ("n", C.c_int32 * 3)]
 
 
+class ImageFilter(C.Structure):
+    _fields_ = [("enabled", C.c_int32), ("cos_min", C.c_float), ("cos_max", C.c_float)]
+
+
 class Params(C.Structure):
     _fields_ = [("device", C.c_int32), ("capacity", C.c_uint32), ("energy_threshold", C.c_float),
                 ("seed", C.c_uint64), ("block_size", C.c_uint32), ("grid_size", C.c_uint32),
@@ -75,7 +79,8 @@ class Params(C.Structure):
                 ("tally_nx", C.c_int32), ("tally_ny", C.c_int32), ("hist_bins", C.c_int32),
                 ("hist_emax", C.c_float), ("max_events", C.c_uint32), ("stream", C.c_void_p),
                 ("physics", PhysicsOpts), ("adjoint", C.c_int32), ("adjoint_w_step", C.c_float),
-                ("deposit_capacity", C.c_uint32), ("deposit_grid", DepositGrid)]
+                ("deposit_capacity", C.c_uint32), ("deposit_grid", DepositGrid),
+                ("image_filter", ImageFilter)]
 
 
 class BatchJob(C.Structure):

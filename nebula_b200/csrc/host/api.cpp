@@ -738,6 +738,14 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 				sp.grid = s->dep_grid.as<double>();
 			}
 		}
+		if (params->image_filter.enabled) {
+			const nbl_image_filter& f = params->image_filter;
+			require(f.cos_min <= f.cos_max && f.cos_min >= -1.0f && f.cos_max <= 1.0f,
+				"image filter needs -1 <= cos_min <= cos_max <= 1");
+			T.filter = 1;
+			T.cos_min = f.cos_min;
+			T.cos_max = f.cos_max;
+		}
 		T.n_bins = params->hist_bins > 0 ? params->hist_bins : 200;
 		T.hist_emax = params->hist_emax > 0 ? params->hist_emax : 1000.0f;
 		s->hist.alloc((size_t)T.n_bins * sizeof(uint32_t));

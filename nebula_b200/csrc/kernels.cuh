@@ -48,6 +48,8 @@ struct Tallies {
 	int32_t nx, ny;          // pixel grid
 	int32_t n_bins;
 	float hist_emax;
+	int32_t filter;          // images count only detections with cos(polar angle) in [cos_min, cos_max]
+	float cos_min, cos_max;
 };
 
 struct StepParams {

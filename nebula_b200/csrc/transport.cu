@@ -331,7 +331,7 @@ __device__ __forceinline__ void deposit(const StepParams& P, bool scat, const El
 		lc.add(CNT_DEPOSITS);
 }
 
-template<bool ADJ, bool BATCH>
+template<bool ADJ, bool BATCH, bool DEP = false>
 __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc,
 	float* s_lane = nullptr)
 {
@@ -502,7 +502,7 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		}
 
 		// energy deposit of a scatter event that changed the energy
-		if (!BATCH && (P.dep || P.grid))
+		if (DEP)
 			deposit(P, (kind == EV_ELASTIC || kind == EV_INELASTIC) && p.E != e_before, p, e_before,
 				P.primaries + rec_index, s_lane + (threadIdx.x & ~31u), lc);
 
@@ -515,7 +515,13 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			} else {
 				const Record36* pr = P.primaries + rec_index;
 				const int px = pr->px, py = pr->py;
-				if (T.se_img && px >= 0 && py >= 0 && px < T.nx && py < T.ny) {
+				bool seen = true;
+				if (T.filter) {
+					// detector acceptance: polar angle of the detected direction to +z
+					const float c = fdf(p.dir.z, __fsqrt_rn(vmag2(p.dir)));
+					seen = c >= T.cos_min && c <= T.cos_max;
+				}
+				if (seen && T.se_img && px >= 0 && py >= 0 && px < T.nx && py < T.ny) {
 					const size_t pix = (size_t)py * T.nx + px;
 					atomicAdd((p.E < 50.0f ? T.se_img : T.bse_img) + pix, 1u);
 					if (ADJ && T.grad_se) {
@@ -640,17 +646,19 @@ __device__ __forceinline__ void flush_counters(const StepParams& P, uint32_t* s_
 // One wavefront iteration per launch (the plain method).  Four resident
 // blocks of 256 threads per SM (at most 64 registers): the kernel is latency
 // bound, so warps in flight matter more than registers.
-template<bool ADJ>
+// DEP: energy deposits on (a separate instantiation, so the plain step keeps
+// none of their code).
+template<bool ADJ, bool DEP>
 __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
-	__shared__ float s_lane[256];
+	__shared__ float s_lane[DEP ? 256 : 1];
 	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
 		s_counters[k] = 0u;
 	__syncthreads();
 	LocalCounters lc{ s_counters };
 	const BatchParams none{};
-	step_iteration<ADJ, false>(P, none, it, lc, s_lane);
+	step_iteration<ADJ, false, DEP>(P, none, it, lc, s_lane);
 	flush_counters(P, s_counters);
 }
 
@@ -716,10 +724,14 @@ __global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const Batc
 
 cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)
 {
-	if (p.adjoint)
-		k_step<true><<<grid, block, 0, s>>>(p, iteration);
-	else
-		k_step<false><<<grid, block, 0, s>>>(p, iteration);
+	const bool dep = p.dep || p.grid;
+	if (p.adjoint) {
+		if (dep) k_step<true, true><<<grid, block, 0, s>>>(p, iteration);
+		else k_step<true, false><<<grid, block, 0, s>>>(p, iteration);
+	} else {
+		if (dep) k_step<false, true><<<grid, block, 0, s>>>(p, iteration);
+		else k_step<false, false><<<grid, block, 0, s>>>(p, iteration);
+	}
 	return cudaGetLastError();
 }
 
@@ -727,7 +739,7 @@ int step_grid_size(int device, int block)
 {
 	int sms = 148, per_sm = 1;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<false>, block, 0);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<false, false>, block, 0);
 	if (per_sm < 1)
 		per_sm = 1;
 	return sms * per_sm;
