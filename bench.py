@@ -38,6 +38,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "primaries/s on 1 B200, plain vs batched; adjoint:forward time at yield err ≤3σ"
 BYTES_PER_EVENT = 96   # 48-byte electron state read + written per event
+# DRAM bytes (read + write) per event of the transport kernel on this workload,
+# from an ncu capture of one whole scan (dram__bytes_read.sum +
+# dram__bytes_write.sum over its 168 launches / its 1.4125e9 flights)
+DRAM_BYTES_PER_EVENT = 89.4
 
 
 def measured_peaks():
@@ -513,7 +517,10 @@ def main():
             "events_per_primary": flights / (n_pri * args.steps),
             "detected_per_primary": detected / (n_pri * args.steps),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": DRAM_BYTES_PER_EVENT * flights / max(iters, 1),
+                         "traffic_unit": "bytes per launch (ncu capture of this workload, %.1f B per event)"
+                                         % DRAM_BYTES_PER_EVENT,
                          "note": "%d B algorithmic per event x %d events / transport-kernel time %.1f ms; "
                                  "peak %s" % (BYTES_PER_EVENT, flights, kernel_ms, peak_kind)},
             "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
