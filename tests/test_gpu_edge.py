@@ -1,0 +1,116 @@
+"""Edge cases of the transport through the C ABI: empty runs, primaries
+outside the domain, stepping a run piecewise, pushing primaries in parts,
+and the documented error statuses (record buffer overflow, event budget,
+NaN state) -- every failure is a status, never a silent result."""
+import numpy as np
+import pytest
+
+import nebula_b200 as nb
+
+pytestmark = pytest.mark.gpu
+
+
+def _slab(inputs):
+    return nb.Geometry.from_tri_file(inputs["slab.tri"]), nb.Material.load(inputs["si.nmat"])
+
+
+def _sorted(rec):
+    return np.sort(rec.view(np.dtype((np.void, 36))).ravel()).tobytes()
+
+
+def test_empty_run(inputs):
+    g, m = _slab(inputs)
+    sim = nb.Simulation(g, [m], capacity=1024, seed=1, tally=(4, 4))
+    sim.run()
+    assert len(sim.flush_detected()) == 0
+    c = sim.counters()
+    assert c["flights"] == 0 and c["primaries_started"] == 0
+    se, bse, hist = sim.tallies()
+    assert se.sum() == 0 and bse.sum() == 0 and hist.sum() == 0
+    sim.close()
+
+
+def test_primaries_outside_the_domain_terminate(inputs):
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    pri = primaries.point_beam(500)
+    pri["pos"][:, 0] = 1.0e5                     # far outside the octree box
+    sim = nb.Simulation(g, [m], capacity=1024, seed=1)
+    sim.push(pri)
+    sim.run()
+    c = sim.counters()
+    assert len(sim.flush_detected()) == 0
+    assert c["primaries_started"] == 500 and c["terminated"] == 500 and c["flights"] == 500
+    sim.close()
+
+
+def test_stepping_and_split_push_equal_one_run(inputs):
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    pri = primaries.point_beam(2000)
+    a = nb.Simulation(g, [m], capacity=1 << 12, seed=9)
+    a.push(pri)
+    a.run()
+    ra = a.flush_detected()
+    b = nb.Simulation(g, [m], capacity=1 << 12, seed=9)
+    b.push(pri[:700])
+    b.push(pri[700:])
+    steps = 0
+    while b.do_iteration(24) > 0:
+        steps += 1
+        assert steps < 10000
+    rb = b.flush_detected()
+    assert steps > 1
+    assert len(ra) > 0 and _sorted(ra) == _sorted(rb)
+    a.close()
+    b.close()
+
+
+def test_record_buffer_overflow_is_an_error(inputs):
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    sim = nb.Simulation(g, [m], capacity=1 << 14, seed=1, record_capacity=16)
+    sim.push(primaries.point_beam(5000))
+    with pytest.raises(nb.NblError) as e:
+        sim.run()
+    assert e.value.status == 6
+    sim.close()
+
+
+def test_event_budget_is_an_error(inputs):
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    sim = nb.Simulation(g, [m], capacity=1024, seed=1, max_events=5)
+    sim.push(primaries.point_beam(100))
+    with pytest.raises(nb.NblError) as e:
+        sim.run()
+    assert e.value.status == 4
+    sim.close()
+
+
+def test_nan_state_is_an_error(inputs):
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    pri = primaries.point_beam(10)
+    pri["E"][3] = np.nan
+    sim = nb.Simulation(g, [m], capacity=1024, seed=1)
+    sim.push(pri)
+    with pytest.raises(nb.NblError) as e:
+        sim.run()
+    assert e.value.status == 5
+    sim.close()
+
+
+def test_reset_gives_the_same_run_again(inputs):
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    pri = primaries.point_beam(1500)
+    sim = nb.Simulation(g, [m], capacity=1 << 12, seed=4, tally=(2, 2))
+    outs = []
+    for _ in range(2):
+        sim.reset()
+        sim.push(pri)
+        sim.run()
+        outs.append((_sorted(sim.flush_detected()), [t.tobytes() for t in sim.tallies()]))
+    assert outs[0] == outs[1]
+    sim.close()
