@@ -277,6 +277,9 @@ def ref():
         L.ref_event.restype = C.c_int
         L.ref_event.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_uint32, C.c_int, C.c_int32,
                                 C.c_uint32, f32p, i32p, f32p, C.c_int, i32p]
+        L.ref_simulate_reseeded.restype = C.c_int64
+        L.ref_simulate_reseeded.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_void_p, C.c_int64,
+                                            C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p]
         L.ref_simulate_deposits.restype = C.c_int64
         L.ref_simulate_deposits.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_void_p, C.c_int64,
                                             C.c_uint32, C.c_float, C.c_void_p, C.c_int64, i64p]
@@ -413,3 +416,15 @@ def ref_simulate_deposits(geom, mats, pri, seed, energy_threshold=0.0, max_recor
     if tot.value > cap:
         raise RuntimeError("deposit buffer too small")
     return out[:n]
+
+
+def ref_simulate_reseeded(geom, mats, pri, base_seed, energy_threshold=0.0, max_records=None):
+    """Reference driver with its generator reseeded per primary (base_seed + i)."""
+    pri = np.ascontiguousarray(pri, PRI_DTYPE)
+    cap = max_records if max_records is not None else max(16, 8 * len(pri) + 1024)
+    out = np.zeros(cap, PRI_DTYPE)
+    tot = C.c_int64(0)
+    hs = (C.c_void_p * len(mats))(*[x.h for x in mats])
+    n = ref().ref_simulate_reseeded(geom.h, hs, len(mats), pri.ctypes.data, len(pri), base_seed, energy_threshold,
+                                    out.ctypes.data, cap, C.byref(tot))
+    return out[:n], tot.value

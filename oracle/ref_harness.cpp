@@ -547,6 +547,49 @@ int64_t ref_simulate(void* gh, void** mats, int n_mat, uint32_t phys, const void
 	}
 }
 
+/* ref_simulate with the driver's generator reseeded for every primary
+ * (seed = base_seed + index), so each primary's cascade has its own mt19937
+ * stream: runs of the same primaries with slightly different material
+ * parameters then share random numbers primary by primary (common random
+ * numbers for finite differences).  Default physics.  Writes the detected
+ * records; returns how many. */
+int64_t ref_simulate_reseeded(void* gh, void** mats, int n_mat, const void* pri_records, int64_t n_pri,
+	uint32_t base_seed, float energy_threshold, void* out_records, int64_t max_records, int64_t* n_total)
+{
+	auto* g = static_cast<ref_geometry*>(gh);
+	std::vector<material_t> materials;
+	for (int i = 0; i < n_mat; ++i)
+		materials.emplace_back(static_cast<ref_material*>(mats[i])->file);
+	intersect_t inter;
+	driver_t d(g->oct, inter, materials, energy_threshold, base_seed);
+	int64_t written = 0, total = 0;
+	const char* in = static_cast<const char*>(pri_records);
+	char* out = static_cast<char*>(out_records);
+	for (int64_t i = 0; i < n_pri; ++i)
+	{
+		d.rand_state = nbl::util::random_generator<false>((uint32_t)(base_seed + (uint32_t)i));
+		float f[7]; int32_t px[2];
+		std::memcpy(f, in + 36 * i, 28);
+		std::memcpy(px, in + 36 * i + 28, 8);
+		particle p{ { f[0], f[1], f[2] }, { f[3], f[4], f[5] }, f[6] };
+		uint32_t tag = 0;
+		d.push(&p, &tag, 1);
+		d.simulate_to_end();
+		d.flush_detected([&](particle q, uint32_t) {
+			if (written < max_records)
+			{
+				float r[7] = { q.pos.x, q.pos.y, q.pos.z, q.dir.x, q.dir.y, q.dir.z, q.kin_energy };
+				std::memcpy(out + 36 * written, r, 28);
+				std::memcpy(out + 36 * written + 28, px, 8);
+				++written;
+			}
+			++total;
+		});
+	}
+	*n_total = total;
+	return written;
+}
+
 /* The reference's energy-deposit driver (energydeposit_cpu_driver.h:44-93),
  * default physics, one driver seeded with `seed`, primaries one at a time as
  * cpu_energydep.cpp:170-205 does on one thread; writes its 28-byte deposit

@@ -82,3 +82,42 @@ def test_torch_autograd_matches_jacobian(problem):
     J = problem.jacobian(th.detach().numpy())
     expect = (J * problem.per_pixel[..., None]).sum((0, 1))
     assert np.allclose(th.grad.numpy(), expect, rtol=1e-9, atol=1e-9)
+
+
+def test_gradients_match_reference_driver_fd(tmp_path):
+    """The adjoint's total SE-yield gradients against central finite
+    differences of the REFERENCE's own CPU driver (tests/golden/
+    make_golden_adjoint.py: same scan, 16 x 16 pixels x 4000 primaries, its
+    mt19937 reseeded per primary so the +- runs share random numbers).  The
+    reference differences carry their own statistical error; the bound is
+    5 % of the difference plus 3 combined standard errors."""
+    from conftest import load_golden
+    from nebula_b200.synth import workloads, geometry, materials, nmat
+    from nebula_b200.torch_adjoint import ScanProblem
+    ref = load_golden("adjoint_ref_fd.npz")
+    nx, per = int(ref["nx"]), int(ref["per_pixel_n"])
+    w = workloads.grating(nx=nx, ny=nx, per_pixel=per)
+    tri = str(tmp_path / "g.tri")
+    geometry.write_tri(tri, w.triangles)
+    ms = []
+    for sp in w.material_specs:
+        pth = str(tmp_path / (sp.name + ".nmat"))
+        nmat.write(pth, materials.build_raw_material(sp))
+        ms.append(nb.Material.load(pth))
+    g = nb.Geometry.from_tri_file(tri)
+    prob = ScanProblem(g, ms, w.primaries, (nx, nx), seed=21, capacity=1 << 20)
+    th0 = prob.theta0().numpy()
+    J = prob.jacobian(th0)
+    W = prob.per_pixel
+    assert np.array_equal(W, ref["per_pixel"])
+    N = W.sum()
+    counts, deltas = ref["counts_se"], ref["deltas"]
+    for k in range(6):
+        adj_pix = J[..., k] * W
+        adj = adj_pix.sum() / N
+        se_adj = adj_pix.std(ddof=1) * np.sqrt(adj_pix.size) / N
+        fd_pix = (counts[k, 1] - counts[k, 0]) / (2 * deltas[k])
+        fd = fd_pix.sum() / N
+        se_fd = fd_pix.std(ddof=1) * np.sqrt(fd_pix.size) / N
+        assert abs(adj - fd) <= 0.05 * abs(fd) + 3 * np.hypot(se_adj, se_fd), (str(ref["params"][k]), adj, fd, se_fd)
+    prob.close()
