@@ -450,10 +450,12 @@ def main():
             sim.run()
 
         def step_e2e():
+            # records stream into the pinned host buffer on a copy stream while
+            # the later iterations run (the record sink)
             sim.reset()
             sim.push(np.frombuffer(pri_host.numpy(), dtype=nb.PRI_DTYPE))
             sim.run()
-            rec = sim.flush_detected(out=rec_view)
+            rec = sim.sink_records()
             tal = sim.tallies()
             return rec, tal
 
@@ -491,6 +493,7 @@ def main():
         d2h = 0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        sim.set_record_sink(rec_view)
         torch.cuda.synchronize(dev)
         e0.record(stream)
         for _ in range(args.steps):

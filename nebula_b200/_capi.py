@@ -142,6 +142,8 @@ _DECLS = [
     ("nbl_sim_get_theta", C.c_int, [C.c_void_p, f32p, C.c_int32]),
     ("nbl_sim_gradients", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("nbl_sim_drain_deposits", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, i64p]),
+    ("nbl_sim_set_record_sink", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    ("nbl_sim_sink_count", C.c_int, [C.c_void_p, i64p]),
     ("nbl_sim_deposit_grid", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_sim_destroy", None, [C.c_void_p]),

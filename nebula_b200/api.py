@@ -362,6 +362,22 @@ class Simulation:
                                       gb.ctypes.data_as(C.POINTER(C.c_double))))
         return gs, gb
 
+    def set_record_sink(self, out):
+        """Stream detected records into ``out`` (a PRI_DTYPE array, ideally in
+        page-locked memory) during later runs; None removes the sink."""
+        if out is None:
+            check(lib().nbl_sim_set_record_sink(self._h, None, 0))
+            self._sink = None
+            return
+        self._sink = out
+        check(lib().nbl_sim_set_record_sink(self._h, out.ctypes.data, len(out)))
+
+    def sink_records(self):
+        """The records streamed into the sink so far (a view of it)."""
+        n = C.c_int64()
+        check(lib().nbl_sim_sink_count(self._h, C.byref(n)))
+        return self._sink[:n.value]
+
     def drain_deposits(self):
         """Energy-deposit records of the run so far (DEPOSIT_DTYPE), removed
         from the simulation."""

@@ -89,8 +89,27 @@ struct nbl_sim {
 	uint32_t record_growth = 0;             // most records one graph has added
 	uint32_t* pinned_ctrl = nullptr;
 
+	// Record sink: page-locked host memory the step kernel writes the detected
+	// records into directly (over the bus, as they are produced), so a run's
+	// output needs no copy after it.
+	nbl_record* sink = nullptr;
+	void* sink_dev = nullptr;               // its device-side address
+	int64_t sink_cap = 0;
+	bool sink_registered = false;           // page-locked by this library
+	uint32_t dev_det_cap = 0;               // capacity of the device record buffer
+
+	void release_sink()
+	{
+		if (sink_registered && sink) cudaHostUnregister(sink);
+		sink_registered = false;
+		sink = nullptr;
+		sink_dev = nullptr;
+		sink_cap = 0;
+	}
+
 	~nbl_sim()
 	{
+		release_sink();
 		if (graph) cudaGraphExecDestroy(graph);
 		if (ev0) cudaEventDestroy(ev0);
 		if (ev1) cudaEventDestroy(ev1);
@@ -184,7 +203,7 @@ struct nbl_sim {
 			const uint32_t ndet = pinned_ctrl[SLOT_WORDS];
 			record_growth = std::max(record_growth, ndet >= records_seen ? ndet - records_seen : ndet);
 			const uint64_t reserve = std::max<uint64_t>(2ull * record_growth, sp.det_cap / 8);
-			if ((uint64_t)ndet + reserve > sp.det_cap) {
+			if (!sink && (uint64_t)ndet + reserve > sp.det_cap) {
 				drain_to_host(ndet);
 				records_seen = 0;
 			} else {
@@ -245,7 +264,7 @@ struct nbl_sim {
 			throw Error(NBL_ERR_POOL_OVERFLOW, std::to_string(cnt[CNT_DEPOSIT_OVERFLOW]) +
 				" deposit records dropped; raise deposit_capacity");
 		if (cnt[CNT_QUEUE_OVERFLOW] || cnt[CNT_RECORD_OVERFLOW])
-			throw Error(NBL_ERR_POOL_OVERFLOW, "secondary overflow ring or record buffer full (" +
+			throw Error(NBL_ERR_POOL_OVERFLOW, "secondary overflow ring, record buffer or record sink full (" +
 				std::to_string(cnt[CNT_QUEUE_OVERFLOW]) + " electrons, " + std::to_string(cnt[CNT_RECORD_OVERFLOW]) +
 				" records dropped); raise capacity / record_capacity");
 		if (cnt[CNT_NAN])
@@ -686,6 +705,7 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		sp.counters = s->counters.as<unsigned long long>();
 		sp.det_cap = params->record_capacity ? params->record_capacity : std::max<uint32_t>(4 * cap, 1u << 20);
 		s->detected.alloc((size_t)sp.det_cap * sizeof(Record36));
+		s->dev_det_cap = sp.det_cap;
 		sp.detected = s->detected.as<Record36>();
 		s->n_detected.alloc(sizeof(uint32_t));
 		sp.n_detected = s->n_detected.as<uint32_t>();
@@ -820,6 +840,58 @@ nbl_status nbl_sim_run(nbl_sim* s)
 	});
 }
 
+nbl_status nbl_sim_set_record_sink(nbl_sim* s, nbl_record* host, int64_t capacity)
+{
+	return guard([&] {
+		require(s != nullptr, "null simulation");
+		require(capacity >= 0 && capacity <= 0xFFFFFFFFll && (host || capacity == 0), "bad record sink");
+		set_device(s->device);
+		CU(cudaStreamSynchronize(s->stream));
+		s->release_sink();
+		if (capacity > 0) {
+			void* dev = nullptr;
+			cudaPointerAttributes a{};
+			if (cudaPointerGetAttributes(&a, host) == cudaSuccess && a.type == cudaMemoryTypeHost && a.devicePointer) {
+				dev = a.devicePointer;
+			} else {
+				cudaGetLastError();
+				const cudaError_t e = cudaHostRegister(host, (size_t)capacity * sizeof(nbl_record),
+					cudaHostRegisterMapped);
+				if (e != cudaSuccess) {
+					cudaGetLastError();
+					throw Error(NBL_ERR_INVALID_ARG, "the record sink could not be page-locked and mapped");
+				}
+				s->sink_registered = true;
+				CU(cudaHostGetDevicePointer(&dev, host, 0));
+			}
+			s->sink = host;
+			s->sink_dev = dev;
+			s->sink_cap = capacity;
+		}
+		// records of later runs go to the sink (or back to the device buffer)
+		s->sp.detected = s->sink ? static_cast<Record36*>(s->sink_dev) : s->detected.as<Record36>();
+		s->sp.det_cap = s->sink ? (uint32_t)s->sink_cap : s->dev_det_cap;
+		s->graph_dirty = true;
+		CU(cudaMemsetAsync(s->n_detected.p, 0, sizeof(uint32_t), s->stream));
+		CU(cudaStreamSynchronize(s->stream));
+		s->records_seen = 0;
+	});
+}
+
+nbl_status nbl_sim_sink_count(nbl_sim* s, int64_t* n)
+{
+	return guard([&] {
+		require(s && n, "null argument");
+		set_device(s->device);
+		uint32_t d = 0;
+		if (s->sink) {
+			CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+			CU(cudaStreamSynchronize(s->stream));
+		}
+		*n = std::min<int64_t>(d, s->sink_cap);
+	});
+}
+
 nbl_status nbl_sim_detected_count(nbl_sim* s, int64_t* n)
 {
 	return guard([&] {
@@ -842,6 +914,11 @@ nbl_status nbl_sim_drain_detected(nbl_sim* s, nbl_record* out, int64_t cap, int6
 		const int64_t k = std::min<int64_t>(cap, (int64_t)s->host_records.size());
 		if (k > 0) std::memcpy(out, s->host_records.data(), (size_t)k * sizeof(nbl_record));
 		s->host_records.erase(s->host_records.begin(), s->host_records.begin() + k);
+		if (s->sink) {
+			// with a record sink every record is already in it
+			*n = k;
+			return;
+		}
 		uint32_t d = 0;
 		CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
 		CU(cudaStreamSynchronize(s->stream));
