@@ -54,7 +54,7 @@ def detector_plane(out, z, half_x, half_y):
 
 
 def slab(size=1000.0, detector_z=10.0):
-    """Config-0 geometry: a ``size``^3 material-0 cube with its top at z=0,
+    """The slab: a ``size``^3 material-0 cube with its top at z=0,
     vacuum outside, and a detector plane at ``detector_z`` over the footprint."""
     h = size / 2
     out = []
@@ -74,7 +74,7 @@ def _line_profile(center, top_cd, height, sidewall_deg):
 def grating(n_lines=8, pitch=32.0, top_cd=16.0, sidewall_deg=86.0, height=30.0,
             size=1000.0, y_segments=50, detector_z=50.0, line_mat=1, sub_mat=0,
             edge_fn=None, z_rows=1, line_length=None):
-    """Config-1 style line-space grating on the config-0 substrate.
+    """Line-space grating of trapezoidal lines on the slab substrate.
 
     Lines run along y, centred on x=0.  Each line is cut into ``y_segments``
     segments along y (and its sidewalls into ``z_rows`` rows) so that the
@@ -170,7 +170,7 @@ def gaussian_random_field_1d(n, spacing, sigma, corr_len, rng):
 def rough_grating(n_lines=16, pitch=32.0, top_cd=16.0, sidewall_deg=86.0, height=30.0,
                   size=1000.0, line_length=500.0, vertex_spacing=0.25, sigma=1.5,
                   corr_len=20.0, z_rows=8, seed=1234, detector_z=50.0):
-    """Config-2 style grating with line-edge roughness (about 1.2 M triangles
+    """Grating with line-edge roughness (about 1.2 M triangles
     at the defaults)."""
     rng = np.random.default_rng(seed)
     nseg = int(round(line_length / vertex_spacing))

@@ -15,7 +15,7 @@ assert PRI_DTYPE.itemsize == 36
 
 def point_beam(n, pos=(0.0, 0.0, 5.0), direction=(0.0, 0.0, -1.0), energy=1000.0,
                pixel=(0, 0)):
-    """``n`` identical primaries (config-0 beam)."""
+    """``n`` identical primaries (a point beam at normal incidence)."""
     rec = np.zeros(n, dtype=PRI_DTYPE)
     rec["pos"] = pos
     rec["dir"] = direction

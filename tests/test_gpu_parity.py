@@ -188,7 +188,7 @@ def _transport_parity(sim, pri, gold, keys):
 
 
 def test_transport_slab_yields_and_distributions(inputs):
-    """Config-0 slab, 10^6 primaries at 1 keV, one pixel per primary."""
+    """Slab, 10^6 primaries at 1 keV, one pixel per primary."""
     gold = load_golden("stats_slab.npz")
     g = nb.Geometry.from_tri_file(inputs["slab.tri"])
     m = nb.Material.load(inputs["si.nmat"])
@@ -203,7 +203,7 @@ def test_transport_slab_yields_and_distributions(inputs):
 
 
 def test_transport_grating_yields_and_distributions(inputs):
-    """Config-1 grating, 100 x 100 pixel subset x 100 primaries at 500 eV."""
+    """Line-space grating, 100 x 100 pixel subset x 100 primaries at 500 eV."""
     gold = load_golden("stats_grating.npz")
     g = nb.Geometry.from_tri_file(inputs["grating.tri"])
     ms = [nb.Material.load(inputs["si.nmat"]), nb.Material.load(inputs["pmma.nmat"])]
