@@ -206,8 +206,9 @@ def reference_arm(args):
 # ---------------------------------------------------------------------------- batch
 def batched_vs_plain(args, dev, workdir):
     """The mixed 64-job batch: one persistent batched launch against the
-    plain wavefront run job by job (one pool reused per geometry; pool
-    creation not timed), same seeds, so per-job yields must be identical.
+    plain wavefront run job by job (one pool reused per geometry, with the
+    plain bench's capacity; pool creation not timed), same seeds, so per-job
+    yields must be identical.
     Batch parameters come from the autotuner's stored choice when present."""
     import torch
     import nebula_b200 as nb
@@ -240,8 +241,8 @@ def batched_vs_plain(args, dev, workdir):
             if cur is None or cur[0] != gi:
                 if cur is not None:
                     cur[1].close()
-                cur = (gi, nb.Simulation(geoms[gi], mats[: (1 if gi == 0 else 2)], capacity=1 << 20, seed=seed,
-                                         record_capacity=1 << 24, device=dev))
+                cur = (gi, nb.Simulation(geoms[gi], mats[: (1 if gi == 0 else 2)], capacity=args.capacity,
+                                         seed=seed, record_capacity=1 << 24, device=dev))
             s = cur[1]
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
