@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libnbl_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libnbl_ref.so")
 REF_CPU_MT = os.path.join(HERE, "_ref", "nebula_cpu_mt")
+REF_GPU = os.path.join(HERE, "_ref", "nebula_gpu")
 
 TABLE_NAMES = ("el_imfp", "el_icdf", "in_imfp", "in_omega", "in_q", "in_binding")
 TABLE_DIMS = (1, 2, 1, 2, 3, 3)
