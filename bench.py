@@ -17,7 +17,9 @@ e2e:   the same through the public API from pinned host records: host->device
 Multi-GPU (torchrun): replicas, one scan per rank with its own seed (weak
 scaling); time = max over ranks.  --impl reference times the reference's own
 multithreaded CPU driver (oracle/_ref/nebula_cpu_mt built from its sources)
-on a bounded sample of the same scan with all host threads.
+on a bounded sample of the same scan with all host threads; its line also
+carries the reference's own GPU driver (oracle/_ref/nebula_gpu, gpu_main.cu
+built for sm_100a) timed on 8 copies of the full scan on one GPU.
 """
 from __future__ import annotations
 
@@ -172,6 +174,54 @@ def cpu_baseline(w, tri, mats, workdir):
             "sample": "%d primaries of the scan, oracle restatement, %d threads" % (len(sample), cores)}
 
 
+def _cuda_visible():
+    # gpu_main.cu never returns without a GPU (it waits for its per-GPU
+    # worker threads), so it is only started where one is visible
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def run_reference_gpu(tri, mats, pri_records, workdir, repeat, device=0):
+    """The reference's own GPU driver (oracle/_ref/nebula_gpu: gpu_main.cu
+    unmodified, built for sm_100a) on `repeat` copies of the given primaries,
+    on one GPU, its records to /dev/null.  Its "Simulation" timer polls once a
+    second, so the rate is also taken from the slope of its per-second
+    progress line (primaries taken from its work pool)."""
+    from oracle import oracle as O
+    pri_path = os.path.join(workdir, "ref_gpu.pri")
+    raw = np.ascontiguousarray(pri_records).tobytes()
+    with open(pri_path, "wb") as f:
+        for _ in range(repeat):
+            f.write(raw)
+    n = repeat * len(pri_records)
+    # one GPU: the device-th of the ones this process may see
+    visible = [x for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=visible[device] if device < len(visible) else str(device))
+    try:
+        with open(os.devnull, "wb") as sink, ClockSampler(device) as clk:
+            r = subprocess.run([O.REF_GPU, tri, pri_path] + mats, stdout=sink, stderr=subprocess.PIPE, text=True,
+                               env=env, timeout=300)
+    finally:
+        os.remove(pri_path)
+    if r.returncode != 0 or "Simulation successful" not in r.stderr:
+        raise RuntimeError(r.stderr[-500:])
+    m = re.search(r"Simulation:\s*([0-9.]+)", r.stderr)
+    sim_s = float(m.group(1))
+    prog = [float(x) for x in re.findall(r"Progress ([0-9.]+)%", r.stderr)]
+    slope = None
+    if len(prog) >= 3:
+        # ticks 1 .. k-1 are one second apart while the pool drains
+        slope = (prog[-2] - prog[0]) / (len(prog) - 2) / 100.0 * n
+    return {"value": slope if slope else n / sim_s, "unit": "primaries/s",
+            "kind": "reference GPU driver (gpu_main.cu unmodified, sm_100a, default capacity 10^6)",
+            "sample": "%d x the 256x256x100 scan (%d primaries), one GPU" % (repeat, n),
+            "simulation_timer_s": sim_s, "rate_from_timer": n / sim_s, "rate_from_progress": slope,
+            "clocks": clk.summary()}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -191,16 +241,26 @@ def reference_arm(args):
             r, s, _ = run_reference_cpu(tri, mats, sample, d)
             rates.append(r)
             secs.append(s)
+        ref_gpu = None
+        if not args.no_reference_gpu and os.path.exists(O.REF_GPU) and _cuda_visible():
+            try:
+                ref_gpu = run_reference_gpu(tri, mats, w.primaries, d, repeat=8,
+                                            device=int(os.environ.get("LOCAL_RANK", "0")))
+            except Exception as e:  # reported, not fatal
+                ref_gpu = {"value": None, "error": str(e)[:300]}
     value = len(sample) * len(secs) / sum(secs)
     desc = "%d pixels x 100 primaries (%d) of the scan per step, reference nebula_cpu_mt, %d threads" % (
         n_pix, len(sample), cores)
-    print(json.dumps({
+    line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "primaries/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(secs)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "grating-256x256x100-500eV (bounded CPU sample)", "sample": desc},
         "cpu_baseline": {"value": value, "unit": "primaries/s", "cores": cores, "kind": "reference", "sample": desc},
-        "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if ref_gpu is not None:
+        line["reference_gpu"] = ref_gpu
+    print(json.dumps(line))
 
 
 # ---------------------------------------------------------------------------- batch
@@ -411,6 +471,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch (batched vs plain) measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint vs forward measurement")
     ap.add_argument("--no-rough", action="store_true", help="skip the large-mesh (rough lines) measurement")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own GPU driver beside its CPU driver")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
