@@ -19,7 +19,8 @@ scaling); time = max over ranks.  --impl reference times the reference's own
 multithreaded CPU driver (oracle/_ref/nebula_cpu_mt built from its sources)
 on a bounded sample of the same scan with all host threads; its line also
 carries the reference's own GPU driver (oracle/_ref/nebula_gpu, gpu_main.cu
-built for sm_100a) timed on 8 copies of the full scan on one GPU.
+built for sm_100a) timed on 8 copies of the full scan on one GPU, and the same
+driver run job after job on the mixed 64-job batch (oracle/_ref/ref_gpu_jobs).
 """
 from __future__ import annotations
 
@@ -222,6 +223,54 @@ def run_reference_gpu(tri, mats, pri_records, workdir, repeat, device=0):
             "clocks": clk.summary()}
 
 
+def run_reference_gpu_jobs(workdir, device=0):
+    """The reference's plain GPU driver job after job on the mixed 64-job
+    batch (oracle/_ref/ref_gpu_jobs: the reference's gpu_driver calls
+    sequenced as gpu_main.cu's worker does -- prescan, then frames -- with
+    per-phase timers instead of its once-a-second poll).  Its run time is the
+    sum of the jobs' prescan and frame phases; driver construction (pool
+    allocation, 10^6 cuRAND states) is reported apart, as pool creation is
+    not timed for the plain kernel either."""
+    from oracle import oracle as O
+    from nebula_b200.synth import workloads, geometry, materials, nmat, primaries
+    gt, specs, jobs, _ = workloads.batch()
+    tris = []
+    for i, t in enumerate(gt):
+        p = os.path.join(workdir, "batch_g%d.tri" % i)
+        geometry.write_tri(p, t)
+        tris.append(p)
+    mats = []
+    for sp in specs:
+        p = os.path.join(workdir, "batch_%s.nmat" % sp.name)
+        nmat.write(p, materials.build_raw_material(sp))
+        mats.append(p)
+    lines = []
+    for k, (gi, seed, pri) in enumerate(jobs):
+        p = os.path.join(workdir, "batch_j%d.pri" % k)
+        primaries.write_pri(p, pri)
+        lines.append("%s %s %d" % (tris[gi], p, seed))
+    jobs_txt = os.path.join(workdir, "batch_jobs.txt")
+    with open(jobs_txt, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    visible = [x for x in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if x.strip()]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=visible[device] if device < len(visible) else str(device))
+    with ClockSampler(device) as clk:
+        r = subprocess.run([O.REF_GPU_JOBS, jobs_txt] + mats, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                           text=True, env=env, timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError((r.stdout + r.stderr)[-500:])
+    per_job = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    n = sum(j["primaries"] for j in per_job)
+    run_s = sum(j["prescan_s"] + j["frames_s"] for j in per_job)
+    return {"value": n / run_s, "unit": "primaries/s",
+            "kind": "reference GPU driver (drivers/gpu/gpu_driver.inl) job after job, gpu_main.cu's worker steps",
+            "workload": "mixed batch: %d jobs, %d primaries" % (len(per_job), n),
+            "seconds": run_s, "construct_seconds": sum(j["construct_s"] for j in per_job),
+            "prescan_seconds": sum(j["prescan_s"] for j in per_job),
+            "se": sum(j["se"] for j in per_job), "bse": sum(j["bse"] for j in per_job),
+            "clocks": clk.summary()}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -248,6 +297,12 @@ def reference_arm(args):
                                             device=int(os.environ.get("LOCAL_RANK", "0")))
             except Exception as e:  # reported, not fatal
                 ref_gpu = {"value": None, "error": str(e)[:300]}
+        ref_gpu_batch = None
+        if not args.no_reference_gpu and os.path.exists(O.REF_GPU_JOBS) and _cuda_visible():
+            try:
+                ref_gpu_batch = run_reference_gpu_jobs(d, device=int(os.environ.get("LOCAL_RANK", "0")))
+            except Exception as e:  # reported, not fatal
+                ref_gpu_batch = {"value": None, "error": str(e)[:300]}
     value = len(sample) * len(secs) / sum(secs)
     desc = "%d pixels x 100 primaries (%d) of the scan per step, reference nebula_cpu_mt, %d threads" % (
         n_pix, len(sample), cores)
@@ -260,6 +315,8 @@ def reference_arm(args):
         "e2e": {"value": value, "unit": "primaries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if ref_gpu is not None:
         line["reference_gpu"] = ref_gpu
+    if ref_gpu_batch is not None:
+        line["reference_gpu_mixed_batch"] = ref_gpu_batch
     print(json.dumps(line))
 
 

@@ -21,6 +21,7 @@ ORACLE_SO = os.path.join(HERE, "libnbl_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libnbl_ref.so")
 REF_CPU_MT = os.path.join(HERE, "_ref", "nebula_cpu_mt")
 REF_GPU = os.path.join(HERE, "_ref", "nebula_gpu")
+REF_GPU_JOBS = os.path.join(HERE, "_ref", "ref_gpu_jobs")
 
 TABLE_NAMES = ("el_imfp", "el_icdf", "in_imfp", "in_omega", "in_q", "in_binding")
 TABLE_DIMS = (1, 2, 1, 2, 3, 3)
