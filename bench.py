@@ -388,6 +388,7 @@ def batched_vs_plain(args, dev, workdir):
             "plain_value": n_pri / pw, "plain_seconds": pw, "plain_transport_seconds": float(np.mean(devs)) / 1e3,
             "ratio_batched_over_plain": pw / bm, "flights": c["flights"], "iterations": c["iterations"],
             "spilled": c["spilled"], "per_job_yields_identical": bool(np.array_equal(se_b, se_p)),
+            "se_total": int(np.sum(se_b)), "bse_total": int(np.sum(bse_b)),
             "params": params, "launches_per_run": 1}
 
 
