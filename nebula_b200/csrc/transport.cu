@@ -31,6 +31,7 @@
 #include "device/physics.cuh"
 
 #include <cooperative_groups.h>
+#include <algorithm>
 namespace cg = cooperative_groups;
 
 #ifndef NBL_STEP_MIN_BLOCKS
@@ -331,10 +332,14 @@ __device__ __forceinline__ void deposit(const StepParams& P, bool scat, const El
 		lc.add(CNT_DEPOSITS);
 }
 
-template<bool ADJ, bool BATCH, bool DEP = false>
+template<bool ADJ, bool BATCH, bool DEP = false, uint32_t PHC = 0u>
 __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc,
 	float* s_lane = nullptr)
 {
+	// physics selection bits: a compile-time constant in the instantiations
+	// for the default selection (its option tests fold away, and the code of
+	// the unselected inelastic model drops out), the run-time word otherwise
+	const uint32_t phys = PHC ? PHC : P.phys;
 	const uint32_t rs = it % 3u, ws = (it + 1u) % 3u, zs = (it + 2u) % 3u;
 	const uint32_t* cr = P.ctrl + rs * SLOT_WORDS;
 	uint32_t* cw = P.ctrl + ws * SLOT_WORDS;
@@ -477,7 +482,7 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			const DevTriangle T = load_tri(rv.geom->tris, last_tri);
 			if (ADJ) {
 				BoundaryScore bs = { 0.0f, 0.0f, -1, -1 };
-				status = boundary_event(T, P.mats, p, mat, r, &bs, P.phys, wshift ? dbar : nullptr);
+				status = boundary_event(T, P.mats, p, mat, r, &bs, phys, wshift ? dbar : nullptr);
 				// the work function enters through barrier = fermi + W of the
 				// materials on either side of the crossing
 				if (!wshift) {
@@ -485,20 +490,20 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 					if (bs.mat_out >= 0 && bs.mat_out < 2) sc[3 * bs.mat_out + 2] += bs.d_out;
 				}
 			} else {
-				status = boundary_event(T, P.mats, p, mat, r, nullptr, P.phys);
+				status = boundary_event(T, P.mats, p, mat, r, nullptr, phys);
 			}
 		} else if (kind == EV_ELASTIC) {
 			lc.add(CNT_ELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
 			r.init(rv.key, event, 1u, stream_tag, lineage);
-			elastic_event(P.mats[mat], p, r, P.phys);
+			elastic_event(P.mats[mat], p, r, phys);
 		} else if (kind == EV_INELASTIC) {
 			lc.add(CNT_INELASTIC);
 			last_tri = -1;
 			PhiloxStream r;
 			r.init(rv.key, event, 1u, stream_tag, lineage);
-			spawn = inelastic_event(P.mats[mat], p, se, r, P.phys);
+			spawn = inelastic_event(P.mats[mat], p, se, r, phys);
 		}
 
 		// energy deposit of a scatter event that changed the energy
@@ -647,8 +652,9 @@ __device__ __forceinline__ void flush_counters(const StepParams& P, uint32_t* s_
 // blocks of 256 threads per SM (at most 64 registers): the kernel is latency
 // bound, so warps in flight matter more than registers.
 // DEP: energy deposits on (a separate instantiation, so the plain step keeps
-// none of their code).
-template<bool ADJ, bool DEP>
+// none of their code).  PHC: nonzero = the physics selection fixed at
+// compile time (PH_DEFAULT only).
+template<bool ADJ, bool DEP, uint32_t PHC = 0u>
 __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
@@ -658,7 +664,7 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 	__syncthreads();
 	LocalCounters lc{ s_counters };
 	const BatchParams none{};
-	step_iteration<ADJ, false, DEP>(P, none, it, lc, s_lane);
+	step_iteration<ADJ, false, DEP, PHC>(P, none, it, lc, s_lane);
 	flush_counters(P, s_counters);
 }
 
@@ -699,7 +705,7 @@ __device__ __forceinline__ bool grid_barrier(const BatchParams& B)
 // batch of jobs, with a grid barrier between iterations instead of a kernel
 // boundary; it ends when an iteration finds no work (all blocks see the same
 // control words) or after max_iterations (error word set).
-template<bool ADJ>
+template<bool ADJ, uint32_t PHC = 0u>
 __global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const BatchParams B)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
@@ -709,7 +715,7 @@ __global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const Batc
 	LocalCounters lc{ s_counters };
 	uint32_t it = 0;
 	for (; it < B.max_iterations; ++it) {
-		if (!step_iteration<ADJ, true>(P, B, it, lc))
+		if (!step_iteration<ADJ, true, false, PHC>(P, B, it, lc))
 			break;
 		if (!grid_barrier(B))
 			break;
@@ -725,11 +731,14 @@ __global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const Batc
 cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)
 {
 	const bool dep = p.dep || p.grid;
+	const bool fixed = p.phys == PH_DEFAULT;
 	if (p.adjoint) {
 		if (dep) k_step<true, true><<<grid, block, 0, s>>>(p, iteration);
+		else if (fixed) k_step<true, false, PH_DEFAULT><<<grid, block, 0, s>>>(p, iteration);
 		else k_step<true, false><<<grid, block, 0, s>>>(p, iteration);
 	} else {
 		if (dep) k_step<false, true><<<grid, block, 0, s>>>(p, iteration);
+		else if (fixed) k_step<false, false, PH_DEFAULT><<<grid, block, 0, s>>>(p, iteration);
 		else k_step<false, false><<<grid, block, 0, s>>>(p, iteration);
 	}
 	return cudaGetLastError();
@@ -749,15 +758,24 @@ int batch_grid_size(int device, int block)
 {
 	int sms = 148, per_sm = 0;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<false>, block, 0);
+	// the cooperative grid must be co-resident for whichever instantiation runs
+	const void* kernels[] = { (const void*)k_batch<false>, (const void*)k_batch<true>,
+		(const void*)k_batch<false, PH_DEFAULT>, (const void*)k_batch<true, PH_DEFAULT> };
+	for (const void* k : kernels) {
+		int n = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, 0);
+		per_sm = per_sm == 0 ? n : std::min(per_sm, n);
+	}
 	return sms * per_sm;
 }
 
 cudaError_t launch_batch(const StepParams& p, const BatchParams& b, int grid, int block, cudaStream_t s)
 {
 	void* args[] = { const_cast<StepParams*>(&p), const_cast<BatchParams*>(&b) };
-	return cudaLaunchCooperativeKernel((const void*)(p.adjoint ? k_batch<true> : k_batch<false>), dim3(grid), dim3(block),
-		args, 0, s);
+	const bool fixed = p.phys == PH_DEFAULT;
+	const void* k = p.adjoint ? (fixed ? (const void*)k_batch<true, PH_DEFAULT> : (const void*)k_batch<true>)
+		: (fixed ? (const void*)k_batch<false, PH_DEFAULT> : (const void*)k_batch<false>);
+	return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(block), args, 0, s);
 }
 
 }  // namespace nbl
