@@ -24,7 +24,15 @@
  *     of written to stdout;
  *   - degenerate prescans of very small jobs are clamped (frame size within
  *     the prescan, batch size within [1, capacity]), where gpu_main.cu would
- *     index past its statistics or divide by zero.
+ *     index past its statistics or divide by zero;
+ *   - the frame loop ends after two consecutive frames that start with
+ *     nothing running and take nothing from the work pool.  gpu_main.cu's own
+ *     test (running_count == 0 && primaries.done(), gpu_main.cu:228-229)
+ *     reads a running count snapshotted before the frame's push, so a frame
+ *     that starts empty and drains the pool into the input buffer ends the
+ *     loop with that batch never simulated -- after the prescan (which leaves
+ *     nothing running) every job whose remaining primaries fit in one batch
+ *     would run its 1 000 prescan primaries only.
  *
  * Usage: ref_gpu_jobs <jobs.txt> <material0> [material1 ...]
  *   jobs.txt: one job per line, "<geometry.tri> <primaries.pri> <seed>".
@@ -144,6 +152,7 @@ int main(int argc, char** argv)
 			// still in the pool and come out with the first flush
 			t0 = std::chrono::steady_clock::now();
 			d.allocate_input_buffers(batch_size);
+			int idle_frames = 0;
 			for (;;) {
 				d.buffer_detected();
 				d.push_to_simulation();
@@ -151,12 +160,15 @@ int main(int argc, char** argv)
 				for (uint32_t i = 0; i < frame_size; ++i)
 					d.do_iteration();
 				iterations += frame_size;
+				const size_t to_go = pool.get_primaries_to_go();
 				d.push_to_buffer(pool);
+				const bool took = pool.get_primaries_to_go() != to_go;
 				const auto running = d.flush_buffered([&](particle p, uint32_t) {
 					if (p.kin_energy < 50) ++n_se; else ++n_bse;
 				});
 				cudaDeviceSynchronize();
-				if (running == 0 && pool.done())
+				idle_frames = (running == 0 && !took && pool.done()) ? idle_frames + 1 : 0;
+				if (idle_frames == 2)
 					break;
 			}
 			frames_s = seconds_since(t0);

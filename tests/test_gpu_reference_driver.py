@@ -12,7 +12,9 @@ statistical:
 * detected energy and polar-angle distributions pass a two-sample KS test at
   p > 0.001 on 20 000-record subsamples;
 * the record layout is the same (the pixel of every record is one of the
-  primaries' pixels).
+  primaries' pixels);
+* the batched kernel's per-job yields on the mixed batch against the same
+  driver run job after job (oracle/_ref/ref_gpu_jobs).
 """
 import os
 import subprocess
@@ -123,3 +125,53 @@ def test_grating_matches_reference_gpu_driver(tmp_path):
     pix = set(zip(w.primaries["px"].tolist(), w.primaries["py"].tolist()))
     assert set(zip(ref["px"].tolist(), ref["py"].tolist())) <= pix
     _compare(ours, ref, 1000)
+
+
+def test_mixed_batch_per_job_matches_reference_gpu_driver(tmp_path):
+    """The batched kernel against the reference's plain GPU driver run job
+    after job (oracle/_ref/ref_gpu_jobs: the reference's gpu_driver calls
+    sequenced as its worker does), on a tenth of the 64-job mixed batch
+    (slab or gratings of pitch 20-64 nm, 200 eV-20 keV): every job's SE and
+    BSE counts within 4.5 Poisson sigma x 1.5 (SE counts are overdispersed),
+    and the batch totals within 3 such sigma."""
+    import json
+    from nebula_b200.synth import workloads, geometry, materials, nmat, primaries
+    if not os.path.exists(O.REF_GPU_JOBS):
+        pytest.skip("reference job harness not built")
+    gt, specs, jobs, desc = workloads.batch(scale=0.1)
+    tris, mats = [], []
+    for i, t in enumerate(gt):
+        p = str(tmp_path / ("g%d.tri" % i))
+        geometry.write_tri(p, t)
+        tris.append(p)
+    for sp in specs:
+        p = str(tmp_path / (sp.name + ".nmat"))
+        nmat.write(p, materials.build_raw_material(sp))
+        mats.append(p)
+    lines = []
+    for k, (gi, seed, pri) in enumerate(jobs):
+        p = str(tmp_path / ("j%d.pri" % k))
+        primaries.write_pri(p, pri)
+        lines.append("%s %s %d" % (tris[gi], p, seed))
+    (tmp_path / "jobs.txt").write_text("\n".join(lines) + "\n")
+    r = subprocess.run([O.REF_GPU_JOBS, str(tmp_path / "jobs.txt")] + mats, stdout=subprocess.PIPE,
+                       stderr=subprocess.PIPE, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-1000:]
+    ref = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(ref) == len(jobs) and all(j["cuda_error"] == 0 for j in ref)
+    assert [j["primaries"] for j in ref] == [len(p) for _, _, p in jobs]
+
+    b = nb.Batch([nb.Geometry.from_tri_file(t) for t in tris], [nb.Material.load(p) for p in mats],
+                 capacity=1 << 21, block_size=512, refill_threshold=0.5)
+    b.set_jobs(jobs)
+    b.run()
+    se, bse = (np.asarray(x, np.int64) for x in b.job_yields())
+    b.close()
+    se_ref = np.array([j["se"] for j in ref])
+    bse_ref = np.array([j["bse"] for j in ref])
+    for name, a, c in (("SE", se, se_ref), ("BSE", bse, bse_ref)):
+        sig = 1.5 * np.sqrt(np.maximum(a + c, 1))
+        z = (a - c) / sig
+        assert np.all(np.abs(z) < 4.5), "%s: job %d ours %d vs reference %d" % (
+            name, int(np.argmax(np.abs(z))), a[np.argmax(np.abs(z))], c[np.argmax(np.abs(z))])
+        assert abs(a.sum() - c.sum()) < 3 * 1.5 * np.sqrt(a.sum() + c.sum())
