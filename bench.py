@@ -460,16 +460,40 @@ def adjoint_vs_forward(args, dev, workdir, nx=64, per_pixel=10_000, fd=True):
 
 
 # ---------------------------------------------------------------------------- rough lines
-def rough_lines(args, dev, workdir, rows=128):
+def device_raster_scan(nx, ny, per_pixel, pixel_size, energy, z0, spot_sigma, seed, dev):
+    """A raster scan built directly in device memory as 36-byte records
+    (pixel-major, ``per_pixel`` primaries per pixel centre with a Gaussian
+    spot, normal incidence): the same layout as the host generator's, random
+    spot offsets from torch's device generator."""
+    import torch
+    n = nx * ny * per_pixel
+    gen = torch.Generator(device=f"cuda:{dev}")
+    gen.manual_seed(seed)
+    words = torch.zeros((n, 9), dtype=torch.float32, device=f"cuda:{dev}")
+    k = torch.arange(n, device=f"cuda:{dev}", dtype=torch.int64) // per_pixel
+    px, py = k % nx, k // nx
+    off = torch.randn((n, 2), generator=gen, device=f"cuda:{dev}", dtype=torch.float32) * spot_sigma
+    words[:, 0] = (px.to(torch.float32) - (nx - 1) / 2.0) * pixel_size + off[:, 0]
+    words[:, 1] = (py.to(torch.float32) - (ny - 1) / 2.0) * pixel_size + off[:, 1]
+    words[:, 2] = z0
+    words[:, 5] = -1.0
+    words[:, 6] = energy
+    iw = words.view(torch.int32)
+    iw[:, 7] = px.to(torch.int32)
+    iw[:, 8] = py.to(torch.int32)
+    del off, k, px, py
+    return words
+
+
+def rough_lines(args, dev, workdir):
     """Large-mesh plain method: the 16-line grating with line-edge roughness
-    (1.2 M triangles, octree depth <= 12, <= 16 triangles per leaf) at 300 eV,
-    200 primaries per pixel over a band of ``rows`` full raster lines of the
-    512 x 512 scan (the throughput per primary of the whole scan; the band
-    keeps the host-side input generation short).  Reports the host octree
-    build time (all host threads) and the device primaries/s."""
+    (1.2 M triangles, octree depth <= 12, <= 16 triangles per leaf), the full
+    512 x 512 pixel scan x 200 primaries at 300 eV (52.4 M primaries, built in
+    device memory).  Reports the host octree build time (all host threads)
+    and the device primaries/s."""
     import torch
     import nebula_b200 as nb
-    from nebula_b200.synth import geometry, materials, nmat, primaries
+    from nebula_b200.synth import geometry, materials, nmat
     t0 = time.perf_counter()
     tri_rows = geometry.rough_grating()
     t_gen = time.perf_counter() - t0
@@ -482,13 +506,10 @@ def rough_lines(args, dev, workdir, rows=128):
         pth = os.path.join(workdir, "rough_" + sp.name + ".nmat")
         nmat.write(pth, materials.build_raw_material(sp))
         ms.append(nb.Material.load(pth))
-    px, py = np.meshgrid(np.arange(512), np.arange(256 - rows // 2, 256 + rows // 2), indexing="xy")
-    pixels = np.stack([px.ravel(), py.ravel()], 1)
-    pri = primaries.raster_scan(512, 512, 200, 0.5, 300.0, 40.0, spot_sigma=1.0, seed=11, pixels=pixels,
-                                pixel_streams=False)
-    n = len(pri)
+    words = device_raster_scan(512, 512, 200, 0.5, 300.0, 40.0, 1.0, 11, dev)
+    n = words.shape[0]
     sim = nb.Simulation(g, ms, capacity=1 << 22, seed=31, record_capacity=1 << 24, tally=(512, 512), device=dev)
-    pri_dev = torch.from_numpy(pri.view(np.uint8)).to(f"cuda:{dev}")
+    pri_dev = words
     sim.reset()
     sim.push_device(pri_dev.data_ptr(), n)
     sim.run()                                          # warm-up
@@ -508,8 +529,8 @@ def rough_lines(args, dev, workdir, rows=128):
     sim.close()
     g.close()
     t = float(np.mean(ms_list)) / 1e3
-    return {"workload": "rough lines: 16 lines, %d triangles, 512 x %d pixels x 200 primaries at 300 eV (%d primaries)"
-                        % (len(tris), rows, n),
+    return {"workload": "rough lines: 16 lines, %d triangles, 512 x 512 pixels x 200 primaries at 300 eV (%d primaries)"
+                        % (len(tris), n),
             "value": n / t, "unit": "primaries/s", "seconds": t, "events_per_primary": flights / n,
             "se_yield": float(se.sum()) / n, "bse_yield": float(bse.sum()) / n,
             "octree_words": int(info["n_octree"]), "octree_build_seconds": t_build,
