@@ -454,6 +454,18 @@ def adjoint_vs_forward(args, dev, workdir, nx=64, per_pixel=10_000, fd=True):
             d = (adj_pix - fd_pix).ravel()
             rows[names[k]] = {"adjoint": float(adj_pix.sum() / N), "crn_fd": float(fd_pix.sum() / N),
                               "sigma_diff": float(d.std(ddof=1) * np.sqrt(n_pix) / N)}
+            # a mean-free-path scale whose 1 % difference is too noisy to
+            # resolve 5 % (standard error above 2.5 % of it) is also
+            # differenced with a 5 % step (5x less noise, O(delta^2) bias)
+            if k % 3 != 2 and rows[names[k]]["sigma_diff"] > 0.025 * abs(rows[names[k]]["crn_fd"]):
+                delta5 = 0.05 * float(th0[k])
+                tp, tm = th0.copy(), th0.copy()
+                tp[k] += delta5
+                tm[k] -= delta5
+                fd5 = (prob.forward(tp) - prob.forward(tm)) * W / (2 * delta5)
+                d5 = (adj_pix - fd5).ravel()
+                rows[names[k]]["crn_fd_5pct"] = float(fd5.sum() / N)
+                rows[names[k]]["sigma_diff_5pct"] = float(d5.std(ddof=1) * np.sqrt(n_pix) / N)
         out["dYse_dtheta"] = rows
     prob.close()
     return out
