@@ -1,0 +1,113 @@
+"""The command-line driver nebula_b200/nebula_b200_gpu, a drop-in for the
+reference's GPU executable (gpu_main.cu): same positional arguments and
+options, 36-byte detected-electron records on stdout.
+
+CPU: usage and argument errors (exit status 1, nothing on stdout), the
+material-count check of gpu_main.cu:322-343.  GPU: the records it writes
+are exactly the records the library's API gives for the same primaries and
+seed (counter-based random numbers make the run independent of how it is
+driven), and its physics switches reach the transport.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import nebula_b200 as nb
+from nebula_b200 import build
+from conftest import has_gpu
+
+DRIVER = build.DRIVER
+
+
+@pytest.fixture(scope="module")
+def driver():
+    if not os.path.exists(DRIVER):
+        build.build()
+    assert os.path.exists(DRIVER)
+    return DRIVER
+
+
+@pytest.fixture(scope="module")
+def slab_files(tmp_path_factory):
+    from nebula_b200.synth import workloads, geometry, materials, nmat, primaries
+    d = tmp_path_factory.mktemp("cli")
+    w = workloads.slab(n_primaries=50_000)
+    tri = str(d / "slab.tri")
+    geometry.write_tri(tri, w.triangles)
+    mat = str(d / "si.nmat")
+    nmat.write(mat, materials.build_raw_material(w.material_specs[0]))
+    pri = str(d / "slab.pri")
+    p = w.primaries.copy()
+    p["px"] = np.arange(len(p)) % 100
+    primaries.write_pri(pri, p)
+    return tri, pri, mat, p
+
+
+def _run(args, timeout=300):
+    return subprocess.run(args, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=timeout)
+
+
+def test_usage_and_bad_arguments(driver, slab_files):
+    tri, pri, mat, _ = slab_files
+    r = _run([driver])
+    assert r.returncode == 1 and r.stdout == b"" and b"Usage: nebula_b200_gpu" in r.stderr
+    r = _run([driver, "--no-such-option", "1", tri, pri, mat])
+    assert r.returncode == 1 and b"unknown option --no-such-option" in r.stderr
+    # the slab needs material 0: none given
+    r = _run([driver, tri, pri])
+    assert r.returncode == 1 and r.stdout == b""
+
+
+def test_not_enough_materials(driver, tmp_path):
+    from nebula_b200.synth import workloads, geometry, materials, nmat, primaries
+    w = workloads.grating(nx=2, ny=2, per_pixel=10)
+    tri = str(tmp_path / "g.tri")
+    geometry.write_tri(tri, w.triangles)
+    mat = str(tmp_path / "si.nmat")
+    nmat.write(mat, materials.build_raw_material(w.material_specs[0]))
+    pri = str(tmp_path / "g.pri")
+    primaries.write_pri(pri, w.primaries)
+    r = _run([driver, tri, pri, mat])
+    assert r.returncode == 1 and b"not enough materials" in r.stderr and r.stdout == b""
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_records_equal_the_api_run(driver, slab_files):
+    tri, pri, mat, p = slab_files
+    r = _run([driver, "--seed", "4242", "--capacity", "65536", tri, pri, mat])
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert b"Simulation successful" in r.stderr and b"Timing (seconds):" in r.stderr
+    got = np.frombuffer(r.stdout, dtype=nb.PRI_DTYPE)
+    sim = nb.Simulation(nb.Geometry.from_tri_file(tri), [nb.Material.load(mat)], capacity=1 << 20, seed=4242)
+    sim.push(p)
+    sim.run()
+    ref = sim.flush_detected()
+    sim.close()
+    key = lambda a: np.sort(a.view(np.dtype((np.void, 36))).ravel()).tobytes()
+    assert len(got) == len(ref) > 0.5 * len(p)
+    assert key(got) == key(ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_physics_switches_and_sorting(driver, slab_files):
+    tri, pri, mat, p = slab_files
+    base = _run([driver, "--seed", "7", tri, pri, mat])
+    assert base.returncode == 0
+    a = np.frombuffer(base.stdout, dtype=nb.PRI_DTYPE)
+    # no secondaries: no SE peak below 50 eV beyond what backscatter leaves
+    nose = _run([driver, "--seed", "7", "--generate-secondaries", "0", tri, pri, mat])
+    assert nose.returncode == 0
+    b = np.frombuffer(nose.stdout, dtype=nb.PRI_DTYPE)
+    assert (b["E"] < 50).sum() < 0.2 * (a["E"] < 50).sum()
+    # sorted primaries: a different assignment of random streams, same physics
+    srt = _run([driver, "--seed", "7", "--sort-primaries", "1", tri, pri, mat])
+    assert srt.returncode == 0
+    c = np.frombuffer(srt.stdout, dtype=nb.PRI_DTYPE)
+    n = len(p)
+    for sel in (lambda x: x["E"] < 50, lambda x: x["E"] >= 50):
+        ya, yc = sel(a).sum(), sel(c).sum()
+        assert abs(ya - yc) < 5 * np.sqrt(2.0 * max(ya, 1)) * 1.5, (ya, yc, n)
