@@ -24,6 +24,8 @@ LIB = os.path.join(HERE, "libnebula_b200.so")
 # the command-line driver (a drop-in for the reference's GPU executable)
 DRIVER_SRC = os.path.join(CSRC, "driver", "nebula_gpu_main.cpp")
 DRIVER = os.path.join(HERE, "nebula_b200_gpu")
+# the same source as the energy-deposit executable
+DRIVER_EDEP = os.path.join(HERE, "nebula_b200_edep")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -82,9 +84,10 @@ def build(verbose=False, force=False) -> str:
     if force or _stale(LIB, objs):
         _run(["g++", "-shared", "-o", LIB] + objs
              + ["-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart_static", "-lpthread", "-ldl", "-lrt"], verbose)
-    if force or _stale(DRIVER, [DRIVER_SRC, LIB] + glob.glob(os.path.join(INCLUDE, "*.h"))):
-        _run(["g++", "-std=c++17", "-O2", "-Wall", "-I" + INCLUDE, DRIVER_SRC, "-o", DRIVER, "-L" + HERE,
-              "-lnebula_b200", "-Wl,-rpath,$ORIGIN", "-pthread"], verbose)
+    for exe, defs in ((DRIVER, []), (DRIVER_EDEP, ["-DNBL_DRIVER_EDEP"])):
+        if force or _stale(exe, [DRIVER_SRC, LIB] + glob.glob(os.path.join(INCLUDE, "*.h"))):
+            _run(["g++", "-std=c++17", "-O2", "-Wall", "-I" + INCLUDE] + defs + [DRIVER_SRC, "-o", exe, "-L" + HERE,
+                  "-lnebula_b200", "-Wl,-rpath,$ORIGIN", "-pthread"], verbose)
     return LIB
 
 

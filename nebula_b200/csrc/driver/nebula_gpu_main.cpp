@@ -12,8 +12,16 @@
 // as run-time switches.  Material files are .nmat (the content of the
 // reference's HDF5 .mat files).
 //
+// Built a second time with NBL_DRIVER_EDEP as nebula_b200_edep, a drop-in
+// for the reference's energy-deposit executable (cpu_energydep.cpp): its
+// options --energy-threshold, --seed, --detect-filename (default
+// detected.bin) and --deposit-filename (default stdout, "stdout" meaning
+// standard output), 28-byte deposit records (position after the event,
+// energy before it, energy lost; pixel: cpu_energydep.cpp:197-204) and the
+// 36-byte detected records.
+//
 // It uses only the C ABI of include/nebula_b200.h.  Differences from the
-// reference driver: no prescan (--prescan-size and --batch-factor are
+// reference drivers: no prescan (--prescan-size and --batch-factor are
 // accepted and ignored: the library keeps its pool full by itself), one
 // device per process (run one process per GPU on disjoint primaries), and
 // every primary is simulated (gpu_main.cu:228-229 can end a run one input
@@ -38,6 +46,14 @@
 #include <vector>
 
 namespace {
+
+#ifdef NBL_DRIVER_EDEP
+constexpr bool kEdep = true;
+constexpr const char* kProgram = "nebula_b200_edep";
+#else
+constexpr bool kEdep = false;
+constexpr const char* kProgram = "nebula_b200_gpu";
+#endif
 
 struct Option {
 	std::string value;
@@ -85,8 +101,8 @@ struct Cli {
 
 	void usage(FILE* f) const
 	{
-		std::fprintf(f, "Usage: nebula_b200_gpu [options] <geometry.tri> <primaries.pri> [material0] .. [materialN]\n"
-			"Options:\n");
+		std::fprintf(f, "Usage: %s [options] <geometry.tri> <primaries.pri> [material0] .. [materialN]\n"
+			"Options:\n", kProgram);
 		for (const auto& kv : opts)
 			std::fprintf(f, "\t--%s: %s [default: %s]\n", kv.first.c_str(), kv.second.help, kv.second.value.c_str());
 	}
@@ -111,6 +127,7 @@ struct Timer {
 };
 
 // Writes record buffers to a stream on its own thread, one at a time.
+template<class T>
 class RecordWriter {
 public:
 	explicit RecordWriter(FILE* f) : f_(f), thread_([this] { loop(); }) {}
@@ -124,7 +141,7 @@ public:
 		thread_.join();
 	}
 	// hand over a buffer; it must not change until wait_idle() returns
-	void submit(const std::vector<nbl_record>* b)
+	void submit(const std::vector<T>* b)
 	{
 		std::unique_lock<std::mutex> l(m_);
 		cv_.wait(l, [this] { return job_ == nullptr; });
@@ -158,12 +175,12 @@ private:
 			cv_.wait(l, [this] { return job_ != nullptr || stop_; });
 			if (job_ == nullptr)
 				return;
-			const std::vector<nbl_record>* b = job_;
+			const std::vector<T>* b = job_;
 			l.unlock();
-			const bool ok = b->empty() || std::fwrite(b->data(), sizeof(nbl_record), b->size(), f_) == b->size();
+			const bool ok = b->empty() || std::fwrite(b->data(), sizeof(T), b->size(), f_) == b->size();
 			l.lock();
 			if (!ok)
-				error_ = "writing records to stdout failed";
+				error_ = "writing records failed";
 			job_ = nullptr;
 			cv_.notify_all();
 		}
@@ -172,7 +189,7 @@ private:
 	FILE* f_;
 	std::mutex m_;
 	std::condition_variable cv_;
-	const std::vector<nbl_record>* job_ = nullptr;
+	const std::vector<T>* job_ = nullptr;
 	bool stop_ = false;
 	std::string error_;
 	std::thread thread_;
@@ -268,6 +285,11 @@ int run(int argc, char** argv)
 	cli.add("seed", "0x78c7e39b", "Random seed");
 	cli.add("sort-primaries", "0", "Sort primary electrons (Morton order of their positions) before simulation");
 	cli.add("device", "0", "CUDA device");
+	if (kEdep) {
+		cli.add("detect-filename", "detected.bin", "Filename for detected electrons");
+		cli.add("deposit-filename", "stdout", "Filename for energy deposits");
+		cli.add("deposit-buffer", "16777216", "Deposit records buffered on the GPU between drains");
+	}
 	cli.add("inelastic-model", "0", "0: full_penn, 1: kieft_inelastic");
 	cli.add("generate-secondaries", "1", "Inelastic events create secondary electrons");
 	cli.add("acoustic-phonon-loss", "1", "kieft_elastic acoustic phonon loss below 200 eV");
@@ -378,48 +400,95 @@ int run(int argc, char** argv)
 	p.physics.quantum_transmission = cli.flag("quantum-transmission");
 	p.physics.interface_refraction = cli.flag("interface-refraction");
 	p.physics.interface_absorption = cli.flag("interface-absorption");
+	if (kEdep)
+		p.deposit_capacity = (uint32_t)cli.u64("deposit-buffer");
 	nbl_sim* sim = nullptr;
 	check(nbl_sim_create(geom, mats.data(), n_mat, &p, &sim), "creating the simulation");
 
-	// the run, records streamed to stdout as it goes (gpu_main.cu:191-231):
-	// each step's records are written by a writer thread while the GPU runs
-	// the next step (two buffers)
+	// output streams: stdout for the detected records (gpu_main.cu) or the
+	// two files of cpu_energydep.cpp:169-170 ("stdout" = standard output)
+	FILE* detect_f = stdout;
+	FILE* deposit_f = nullptr;
+	auto open_out = [](const std::string& name) {
+		if (name == "stdout") return stdout;
+		FILE* f = std::fopen(name.c_str(), "wb");
+		if (!f) throw std::runtime_error("cannot open " + name + " for writing");
+		return f;
+	};
+	if (kEdep) {
+		detect_f = open_out(cli.get("detect-filename"));
+		deposit_f = open_out(cli.get("deposit-filename"));
+	}
+
+	// the run, records streamed out as it goes (gpu_main.cu:191-231): each
+	// step's records are written by writer threads while the GPU runs the
+	// next step
 	timer.start();
 	check(nbl_sim_push_primaries(sim, pri, n_pri), "pushing primaries");
 	nbl_free(pri);
-	RecordWriter writer(stdout);
-	std::vector<nbl_record> buf[2];
-	int cur = 0;
-	int64_t written = 0;
-	auto drain = [&](std::vector<nbl_record>& out) {
-		int64_t pending = 0;
-		check(nbl_sim_detected_count(sim, &pending), "record count");
-		out.resize((size_t)pending);
-		int64_t got = 0;
-		while (got < pending) {
-			int64_t n = 0;
-			check(nbl_sim_drain_detected(sim, out.data() + got, pending - got, &n), "draining records");
-			if (n == 0) break;
-			got += n;
+	int64_t written = 0, deposited = 0;
+	{
+		RecordWriter<nbl_record> writer(detect_f);
+		RecordWriter<nbl_deposit_record> dep_writer(deposit_f ? deposit_f : stdout);
+		std::vector<nbl_record> buf[2];
+		std::vector<nbl_deposit_record> dbuf[2];
+		int cur = 0;
+		auto drain = [&](std::vector<nbl_record>& out) {
+			int64_t pending = 0;
+			check(nbl_sim_detected_count(sim, &pending), "record count");
+			out.resize((size_t)pending);
+			int64_t got = 0;
+			while (got < pending) {
+				int64_t n = 0;
+				check(nbl_sim_drain_detected(sim, out.data() + got, pending - got, &n), "draining records");
+				if (n == 0) break;
+				got += n;
+			}
+			out.resize((size_t)got);
+			written += got;
+		};
+		auto drain_deposits = [&](std::vector<nbl_deposit_record>& out) {
+			nbl_counters c;
+			check(nbl_sim_counters(sim, &c), "counters");
+			out.resize((size_t)c.deposits_pending);
+			int64_t got = 0;
+			while (got < (int64_t)out.size()) {
+				int64_t n = 0;
+				check(nbl_sim_drain_deposits(sim, out.data() + got, (int64_t)out.size() - got, &n), "draining deposits");
+				if (n == 0) break;
+				got += n;
+			}
+			out.resize((size_t)got);
+			deposited += got;
+		};
+		int64_t running = 1;
+		while (running > 0) {
+			check(nbl_sim_step(sim, 240, &running), "transport");
+			writer.wait_idle();             // the other buffers are free again
+			drain(buf[cur]);
+			writer.submit(&buf[cur]);
+			if (kEdep) {
+				dep_writer.wait_idle();
+				drain_deposits(dbuf[cur]);
+				dep_writer.submit(&dbuf[cur]);
+			}
+			cur ^= 1;
+			nbl_counters c;
+			check(nbl_sim_counters(sim, &c), "counters");
+			std::fprintf(stderr, " \rProgress %.2f%% | Running: %lld",
+				100.0 * (double)c.primaries_started / (double)std::max<int64_t>(n_pri, 1), (long long)running);
 		}
-		out.resize((size_t)got);
-		written += got;
-	};
-	int64_t running = 1;
-	while (running > 0) {
-		check(nbl_sim_step(sim, 240, &running), "transport");
-		writer.wait_idle();                 // the other buffer is free again
-		drain(buf[cur]);
-		writer.submit(&buf[cur]);
-		cur ^= 1;
-		nbl_counters c;
-		check(nbl_sim_counters(sim, &c), "counters");
-		std::fprintf(stderr, " \rProgress %.2f%% | Running: %lld",
-			100.0 * (double)c.primaries_started / (double)std::max<int64_t>(n_pri, 1), (long long)running);
+		writer.finish();
+		if (kEdep)
+			dep_writer.finish();
 	}
-	writer.finish();
+	if (detect_f != stdout) std::fclose(detect_f);
+	if (deposit_f && deposit_f != stdout) std::fclose(deposit_f);
 	timer.stop("Simulation");
-	std::fprintf(stderr, "\nSimulation successful!\n%lld detected electrons written.\n\n", (long long)written);
+	std::fprintf(stderr, "\nSimulation successful!\n%lld detected electrons written.\n", (long long)written);
+	if (kEdep)
+		std::fprintf(stderr, "%lld energy deposits written.\n", (long long)deposited);
+	std::fprintf(stderr, "\n");
 	timer.print(stderr);
 
 	nbl_sim_destroy(sim);

@@ -1,6 +1,8 @@
-"""The command-line driver nebula_b200/nebula_b200_gpu, a drop-in for the
+"""The command-line drivers: nebula_b200/nebula_b200_gpu, a drop-in for the
 reference's GPU executable (gpu_main.cu): same positional arguments and
-options, 36-byte detected-electron records on stdout.
+options, 36-byte detected-electron records on stdout; and
+nebula_b200/nebula_b200_edep, the same for its energy-deposit executable
+(cpu_energydep.cpp): 28-byte deposit records and a detected-record file.
 
 CPU: usage and argument errors (exit status 1, nothing on stdout), the
 material-count check of gpu_main.cu:322-343.  GPU: the records it writes
@@ -111,3 +113,36 @@ def test_physics_switches_and_sorting(driver, slab_files):
     for sel in (lambda x: x["E"] < 50, lambda x: x["E"] >= 50):
         ya, yc = sel(a).sum(), sel(c).sum()
         assert abs(ya - yc) < 5 * np.sqrt(2.0 * max(ya, 1)) * 1.5, (ya, yc, n)
+
+
+def test_edep_usage(driver):
+    edep = build.DRIVER_EDEP
+    assert os.path.exists(edep)
+    r = _run([edep])
+    assert r.returncode == 1 and b"Usage: nebula_b200_edep" in r.stderr
+    assert b"--deposit-filename" in r.stderr and b"--detect-filename" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_edep_outputs_equal_the_api_run(driver, slab_files, tmp_path):
+    """nebula_b200_edep (cpu_energydep.cpp's command line): the deposit
+    stream (default stdout) and the detected file are exactly the API's
+    deposit records and detected records of the same run."""
+    tri, pri, mat, p = slab_files
+    det = str(tmp_path / "det.bin")
+    r = _run([build.DRIVER_EDEP, "--seed", "99", "--detect-filename", det, tri, pri, mat])
+    assert r.returncode == 0, r.stderr[-2000:]
+    dep = np.frombuffer(r.stdout, dtype=nb.DEPOSIT_DTYPE)
+    got_det = np.fromfile(det, dtype=nb.PRI_DTYPE)
+    sim = nb.Simulation(nb.Geometry.from_tri_file(tri), [nb.Material.load(mat)], capacity=1 << 20, seed=99,
+                        deposit_capacity=1 << 24)
+    sim.push(p)
+    sim.run()
+    ref_dep = sim.drain_deposits()
+    ref_det = sim.flush_detected()
+    sim.close()
+    key = lambda a, n: np.sort(a.view(np.dtype((np.void, n))).ravel()).tobytes()
+    assert len(dep) == len(ref_dep) > 10 * len(p)
+    assert key(dep, 28) == key(ref_dep, 28)
+    assert key(got_det, 36) == key(ref_det, 36)
