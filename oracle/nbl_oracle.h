@@ -1,7 +1,8 @@
 /*
  * Test infrastructure (oracle), not product code: a CPU restatement of the
  * reference's electron-transport path, used only by tests/, smoke() and
- * bench.py's CPU baseline as the checker.  Nothing in nebula_b200/ links it.
+ * bench.py's CPU baseline, as the model results are compared against.
+ * Nothing in nebula_b200/ links it.
  *
  * It restates, operation by operation and in float32 like the reference's
  * CPU build (config/config.h:13), the functions its CPU driver runs:

@@ -2,7 +2,7 @@
 
 ctypes bindings for
   * ``libnbl_oracle.so`` -- the CPU restatement of the reference path
-    (oracle/nbl_oracle.cpp), the checker the parity tests use;
+    (oracle/nbl_oracle.cpp), the model the parity tests compare against;
   * ``_ref/libnbl_ref.so`` -- the reference's own code compiled from its
     sources (oracle/ref_harness.cpp), used to pin the restatement and to make
     golden fixtures; optional (absent where the reference sources are not).

@@ -1,10 +1,10 @@
-"""This build against the reference's own GPU driver run on the same B200.
+"""The CUDA path against the reference's own GPU driver run on the same B200.
 
 oracle/_ref/nebula_gpu is the reference's gpu_main.cu, unmodified, compiled
 for sm_100a from its sources (oracle/Makefile, target ref-gpu).  It runs as a
 separate process on the same inputs (.tri, .pri, material files) and writes
 its 36-byte detected-electron records to stdout (gpu_main.cu:216-223).  Its
-random numbers (cuRAND XORWOW) differ from this build's, so the comparison is
+random numbers (cuRAND XORWOW) differ from the library's (Philox), so the comparison is
 statistical:
 
 * SE and BSE yields agree within 4 sigma, sigma from the spread of per-pixel
