@@ -260,6 +260,15 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 nbl_status nbl_sim_push_primaries(nbl_sim* s, const nbl_record* recs, int64_t n);
 /* Same from device memory (records already resident in HBM). */
 nbl_status nbl_sim_push_primaries_device(nbl_sim* s, const void* d_recs, int64_t n);
+/* Index of the first primary pushed within a larger scan (default 0).  A
+ * primary's random numbers are keyed by the seed and this index, so a scan
+ * resumed at primary k (first = k, pushing primaries k..) or split over
+ * devices (each with its range's first index) gives exactly the records the
+ * whole scan gives in one run (work_pool's primary cursor, work_pool.h:69-88,
+ * made reproducible).  Only while no primaries are queued (after create or
+ * reset); it stays set across nbl_sim_reset; first + primaries pushed must
+ * stay below 2^32. */
+nbl_status nbl_sim_set_primary_offset(nbl_sim* s, uint64_t first);
 /* Run `iterations` wavefront iterations (rounded up to whole graphs); the
  * number still in flight or queued is returned (gpu_driver::do_iteration,
  * get_running_count). */

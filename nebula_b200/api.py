@@ -282,6 +282,12 @@ class Simulation:
     def push_device(self, ptr, n):
         check(lib().nbl_sim_push_primaries_device(self._h, C.c_void_p(ptr), n))
 
+    def set_primary_offset(self, first):
+        """Index of the first primary pushed within a larger scan: a resumed
+        or sharded scan then gives exactly the whole scan's records.  Only
+        while no primaries are queued (after creation or reset())."""
+        check(lib().nbl_sim_set_primary_offset(self._h, int(first)))
+
     # gpu_driver::do_iteration (rounded up to whole graphs)
     def do_iteration(self, n=1):
         running = C.c_int64()

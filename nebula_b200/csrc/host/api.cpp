@@ -785,6 +785,8 @@ static void push_common(nbl_sim* s, const void* src, int64_t n, cudaMemcpyKind k
 	require(s != nullptr, "null simulation");
 	require(n >= 0, "negative count");
 	require(s->n_pri + (uint64_t)n < 0xFFFFFFFFull, "at most 2^32-1 primaries per simulation");
+	require(s->sp.tag_base + s->n_pri + (uint64_t)n <= 0xFFFFFFFFull,
+		"primary offset + primaries must stay below 2^32");
 	if (n == 0) return;
 	set_device(s->device);
 	s->ensure_primary_capacity(s->n_pri + n);
@@ -800,6 +802,17 @@ nbl_status nbl_sim_push_primaries(nbl_sim* s, const nbl_record* recs, int64_t n)
 	return guard([&] {
 		require(recs != nullptr || n == 0, "null records");
 		push_common(s, recs, n, cudaMemcpyHostToDevice);
+	});
+}
+
+nbl_status nbl_sim_set_primary_offset(nbl_sim* s, uint64_t first)
+{
+	return guard([&] {
+		require(s != nullptr, "null simulation");
+		require(s->n_pri == 0, "the primary offset is set while no primaries are queued (after create or reset)");
+		require(first < 0xFFFFFFFFull, "the primary offset must be below 2^32 - 1");
+		s->sp.tag_base = (uint32_t)first;
+		s->graph_dirty = true;
 	});
 }
 

@@ -67,6 +67,7 @@ struct StepParams {
 	uint32_t* ctrl;           // 3 slots x SLOT_WORDS
 	const Record36* primaries;
 	uint32_t n_primaries;
+	uint32_t tag_base;        // random-stream tag of primaries[0] (a resumed or sharded scan)
 	Record36* detected;
 	uint32_t* n_detected;
 	uint32_t det_cap;

@@ -437,7 +437,7 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 				const uint32_t j = job_of(B, qi);
 				tag = (j << 24) | (qi - __ldg(&B.jobs[j].first));
 			} else {
-				tag = qi;
+				tag = P.tag_base + qi;
 			}
 			lc.add(CNT_PRIMARIES);
 		}
@@ -445,7 +445,7 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		// run context: job geometry / key, the primary's record, the tag that
 		// keys the random numbers
 		RunView rv;
-		uint32_t job = 0, stream_tag = tag, rec_index = tag;
+		uint32_t job = 0, stream_tag = tag, rec_index = BATCH ? tag : tag - P.tag_base;
 		if (BATCH) {
 			job = tag >> 24;
 			stream_tag = tag & 0xFFFFFFu;

@@ -201,3 +201,56 @@ def test_distinct_handles_run_concurrently_from_host_threads(inputs):
         t.join()
     assert not errors, errors
     assert together == alone
+
+
+def test_resumed_and_sharded_scans_give_the_whole_scans_records(inputs):
+    """A primary's random numbers are keyed by its index in the scan: a scan
+    resumed at primary k (offset k) or split into shards (each with its first
+    index) gives exactly the records of the whole scan run at once, on any
+    capacity; without the offset a resumed part would reuse the first
+    primaries' streams."""
+    from nebula_b200.synth import primaries
+    from nebula_b200 import replicas
+    g = nb.Geometry.from_tri_file(inputs["grating.tri"])
+    ms = [nb.Material.load(inputs["si.nmat"]), nb.Material.load(inputs["pmma.nmat"])]
+    pri = primaries.raster_scan(24, 24, 50, 0.5, 500.0, 40.0, spot_sigma=1.0, seed=8)
+    n = len(pri)
+    whole = nb.Simulation(g, ms, capacity=1 << 15, seed=55)
+    whole.push(pri)
+    whole.run()
+    ref = whole.flush_detected()
+    whole.close()
+    sim = nb.Simulation(g, ms, capacity=1 << 12, seed=55)
+    # resumed at k
+    k = 10_007
+    resumed = []
+    for first, chunk in ((0, pri[:k]), (k, pri[k:])):
+        sim.reset()
+        sim.set_primary_offset(first)
+        sim.push(chunk)
+        sim.run()
+        resumed.append(sim.flush_detected())
+    assert _sorted(np.concatenate(resumed)) == _sorted(ref)
+    # three shards, as the replicas would take them
+    parts = []
+    for rank in range(3):
+        lo, hi = replicas.shard(n, rank, 3)
+        sim.reset()
+        sim.set_primary_offset(lo)
+        sim.push(pri[lo:hi])
+        sim.run()
+        parts.append(sim.flush_detected())
+    assert _sorted(np.concatenate(parts)) == _sorted(ref)
+    # the offset is refused while primaries are queued
+    sim.reset()
+    sim.set_primary_offset(0)
+    sim.push(pri[:10])
+    with pytest.raises(nb.NblError):
+        sim.set_primary_offset(5)
+    # without the offset the second part runs on the first primaries' streams
+    sim.reset()
+    sim.set_primary_offset(0)
+    sim.push(pri[k:])
+    sim.run()
+    assert _sorted(sim.flush_detected()) != _sorted(resumed[1])
+    sim.close()
