@@ -285,6 +285,8 @@ int run(int argc, char** argv)
 	cli.add("seed", "0x78c7e39b", "Random seed");
 	cli.add("sort-primaries", "0", "Sort primary electrons (Morton order of their positions) before simulation");
 	cli.add("device", "0", "CUDA device");
+	cli.add("first-primary", "0", "Index of the file's first primary within a larger scan (resume, or one process "
+		"per GPU on disjoint files: the records equal one run over the whole scan)");
 	if (kEdep) {
 		cli.add("detect-filename", "detected.bin", "Filename for detected electrons");
 		cli.add("deposit-filename", "stdout", "Filename for energy deposits");
@@ -424,6 +426,7 @@ int run(int argc, char** argv)
 	// step's records are written by writer threads while the GPU runs the
 	// next step
 	timer.start();
+	check(nbl_sim_set_primary_offset(sim, cli.u64("first-primary")), "primary offset");
 	check(nbl_sim_push_primaries(sim, pri, n_pri), "pushing primaries");
 	nbl_free(pri);
 	int64_t written = 0, deposited = 0;

@@ -146,3 +146,22 @@ def test_edep_outputs_equal_the_api_run(driver, slab_files, tmp_path):
     assert len(dep) == len(ref_dep) > 10 * len(p)
     assert key(dep, 28) == key(ref_dep, 28)
     assert key(got_det, 36) == key(ref_det, 36)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_split_files_with_first_primary_equal_one_run(driver, slab_files, tmp_path):
+    """Two processes on the two halves of the primaries, the second with
+    --first-primary, write together exactly the records of one run."""
+    from nebula_b200.synth import primaries
+    tri, pri, mat, p = slab_files
+    k = len(p) // 2 + 3
+    a, b = str(tmp_path / "a.pri"), str(tmp_path / "b.pri")
+    primaries.write_pri(a, p[:k])
+    primaries.write_pri(b, p[k:])
+    whole = _run([driver, "--seed", "5", tri, pri, mat])
+    ra = _run([driver, "--seed", "5", tri, a, mat])
+    rb = _run([driver, "--seed", "5", "--first-primary", str(k), tri, b, mat])
+    assert whole.returncode == ra.returncode == rb.returncode == 0
+    key = lambda buf: np.sort(np.frombuffer(buf, dtype=np.dtype((np.void, 36)))).tobytes()
+    assert key(ra.stdout + rb.stdout) == key(whole.stdout)
