@@ -81,15 +81,33 @@ static uint32_t mt_next(orc_rng* r)
 	return y;
 }
 
-extern "C" orc_rng* orc_rng_mt(uint32_t seed)
+static void mt_seed(orc_rng* r, uint32_t seed)
 {
-	orc_rng* r = new orc_rng();
 	r->kind = 0;
 	r->mt[0] = seed;
 	for (int i = 1; i < 624; ++i)
 		r->mt[i] = 1812433253u * (r->mt[i - 1] ^ (r->mt[i - 1] >> 30)) + (uint32_t)i;
 	r->mti = 624;
+}
+
+extern "C" orc_rng* orc_rng_mt(uint32_t seed)
+{
+	orc_rng* r = new orc_rng();
+	mt_seed(r, seed);
 	return r;
+}
+
+// Seed of primary i in the multithreaded loops: the splitmix64 finaliser
+// (Steele, Lea and Flood 2014) of the run seed and the primary index, so a
+// primary's random numbers depend on neither the thread that takes it nor
+// the thread count.
+static uint32_t primary_seed(uint32_t seed, int64_t i)
+{
+	uint64_t z = (uint64_t)seed * 0x9E3779B97F4A7C15ull + (uint64_t)i;
+	z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+	z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+	z ^= z >> 31;
+	return (uint32_t)(z ^ (z >> 32));
 }
 extern "C" orc_rng* orc_rng_list(const float* u, int64_t n)
 {
@@ -1099,6 +1117,8 @@ extern "C" int64_t orc_simulate_deposits(const orc_geometry* g, const orc_materi
 			for (;;) {
 				const int64_t i = cursor++;
 				if (i >= n_pri) break;
+				if (n_threads > 1)
+					mt_seed(rng, primary_seed(seed, i));
 				float f[7];
 				std::memcpy(f, in + 36 * i, 28);
 				std::memcpy(px, in + 36 * i + 28, 8);
@@ -1137,6 +1157,7 @@ extern "C" int64_t orc_simulate_mt(const orc_geometry* g, const orc_material* ma
 			for (;;) {
 				const int64_t i = cursor++;
 				if (i >= n_pri) break;
+				mt_seed(rng, primary_seed(seed, i));
 				float f[7]; int32_t px[2];
 				std::memcpy(f, in + 36 * i, 28);
 				std::memcpy(px, in + 36 * i + 28, 8);

@@ -94,16 +94,19 @@ int64_t orc_simulate(const orc_geometry* g, const orc_material* mats, int n_mat,
 	const void* pri, int64_t n_pri, uint32_t seed, float energy_threshold,
 	void* out, int64_t max_out, int64_t* n_total, int64_t* n_events);
 
-/* Same loop over `n_threads` threads, each with its own mt19937 seeded from a
- * master mt19937(seed) like cpu_mt_main.cpp:79,210, pulling one primary at a
- * time.  Output order is not deterministic.  Returns records written. */
+/* Same loop over `n_threads` threads pulling one primary at a time, the
+ * mt19937 reseeded for every primary from (seed, primary index), so the set
+ * of records depends on neither the thread count nor the scheduling (the
+ * reference's cpu_mt_main.cpp:79,210 gives each thread one stream instead,
+ * which makes its runs irreproducible).  Output order is not deterministic.
+ * Returns records written. */
 int64_t orc_simulate_mt(const orc_geometry* g, const orc_material* mats, int n_mat,
 	const void* pri, int64_t n_pri, uint32_t seed, float energy_threshold, int n_threads,
 	void* out, int64_t max_out, int64_t* n_total, int64_t* n_events);
 
 /* The energy-deposit driver loop (energydeposit_cpu_driver.h:44-93) over
  * `n_threads` threads (1: the primaries in order with mt19937(seed), as the
- * reference run on one thread; more: per-thread seeds as orc_simulate_mt).
+ * reference run on one thread; more: reseeded per primary as orc_simulate_mt).
  * Writes 28-byte deposit records (after.pos, before.E, before.E - after.E,
  * pixel) for every scatter event that changed the energy; returns records
  * written, *n_total all of them. */
