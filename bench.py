@@ -79,7 +79,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *a):
         if self.proc:
@@ -89,10 +89,14 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, t0=None, t1=None):
+        """Median SM clock, its maximum and the throttle reasons seen in the
+        samples taken between t0 and t1 (time.time(); default: all)."""
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if (t0 is not None and ts < t0) or (t1 is not None and ts > t1):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 8:
                 continue
@@ -604,8 +608,8 @@ def main():
             sim.run()
 
         def step_e2e():
-            # records stream into the pinned host buffer on a copy stream while
-            # the later iterations run (the record sink)
+            # the kernel writes the detected records straight into the pinned
+            # host buffer as it finds them (the record sink)
             sim.reset()
             sim.push(np.frombuffer(pri_host.numpy(), dtype=nb.PRI_DTYPE))
             sim.run()
@@ -613,6 +617,11 @@ def main():
             tal = sim.tallies()
             return rec, tal
 
+        # clocks are sampled from the warm-up on (nvidia-smi takes a moment to
+        # start); the line reports the samples inside the timed region, or
+        # those of warm-up and timed region together when it is too short
+        clk = ClockSampler(dev).__enter__()
+        t_warm = time.time()
         for _ in range(args.warmup):
             step_device()
         torch.cuda.synchronize(dev)
@@ -626,8 +635,9 @@ def main():
         flights = 0
         iters = 0
         detected = 0
-        with ClockSampler(dev) as clk:
+        try:
             torch.cuda.synchronize(dev)
+            t_timed = time.time()
             ev0.record(stream)
             for _ in range(args.steps):
                 step_device()
@@ -638,6 +648,14 @@ def main():
                 detected += c["detected"]
             ev1.record(stream)
             torch.cuda.synchronize(dev)
+            t_end = time.time()
+        finally:
+            clk.__exit__(None, None, None)
+        clocks = clk.summary(t_timed, t_end)
+        clocks["window"] = "timed region"
+        if clocks["samples"] < 3:
+            clocks = clk.summary(t_warm, t_end)
+            clocks["window"] = "warm-up and timed region"
         ms = ev0.elapsed_time(ev1)
         if dist:
             ms = replicas.max_over_ranks(ms, dist, device=f"cuda:{dev}")
@@ -682,7 +700,7 @@ def main():
                                  "peak %s" % (BYTES_PER_EVENT, flights, kernel_ms, peak_kind)},
             "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": iters,
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         sim.close()
         if not args.no_batch:
