@@ -11,8 +11,17 @@ and its full secondary cascade.
 value: primaries/s with the primary records already in HBM when the timed
        region starts (a device-to-device push, then the run).
 e2e:   the same through the public API from pinned host records: host->device
-       copy of the primaries, the run, device->host copy of every detected
-       36-byte record and of the tallies, all inside the timed region.
+       copy of the primaries, the run (the kernel writes every detected
+       36-byte record into a pinned host buffer as it finds it), and the
+       device->host copy of the tallies, all inside the timed region.
+
+The same line also carries: the mixed 64-job batch, batched kernel against
+the plain kernel job after job (``batched``); the seed-replay adjoint against
+the forward run on the 64 x 64 x 10^4 grating scan, with finite differences
+(``adjoint``); the full 512 x 512 x 200 rough-lines scan on its 1.2 M-triangle
+mesh (``rough_lines``); the reference CPU driver on a bounded sample
+(``cpu_baseline``); the transport kernel's roofline (``roofline``) and the
+SM clocks sampled during the timed region (``clocks``).
 
 Multi-GPU (torchrun): replicas, one scan per rank with its own seed (weak
 scaling); time = max over ranks.  --impl reference times the reference's own
