@@ -4,7 +4,10 @@
 line-space grating scan (the 4 144-triangle, 8-line PMMA-on-Si grating) on a
 ``pixels x pixels`` block of the 256 x 256 raster at 500 eV, ``--repeat``
 times after one warm-up run, and prints one JSON line with the transport
-kernel time, primaries/s and events per primary.  It is small enough for a
+kernel time, primaries/s and events per primary.  ``--workload rough`` runs
+the 16 rough lines (1.2 M triangles, octree depth <= 12) on a ``pixels x
+pixels`` block at the centre of their 512 x 512 raster (300 eV unless
+``--energy`` is given); ``--workload slab`` the 1 um Si slab.  It is small enough for a
 full ncu capture of a few launches (``-k regex:k_step -s <n> -c <m>``) and
 keeps its whole state on one GPU.
 """
@@ -25,7 +28,7 @@ def main(argv=None):
     ap.add_argument("--capacity", type=int, default=1 << 18)
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--seed", type=int, default=3)
-    ap.add_argument("--workload", default="grating", choices=["grating", "slab"])
+    ap.add_argument("--workload", default="grating", choices=["grating", "slab", "rough"])
     ap.add_argument("--block", type=int, default=0, help="threads per block of the step kernel (0: default)")
     args = ap.parse_args(argv)
 
@@ -38,16 +41,24 @@ def main(argv=None):
             px = np.arange(128 - args.pixels // 2, 128 - args.pixels // 2 + args.pixels)
             pixels = np.stack(np.meshgrid(px, px, indexing="xy"), -1).reshape(-1, 2)
             w = workloads.grating(pixels=pixels, per_pixel=args.per_pixel, energy=args.energy)
+        elif args.workload == "rough":
+            px = np.arange(256 - args.pixels // 2, 256 - args.pixels // 2 + args.pixels)
+            pixels = np.stack(np.meshgrid(px, px, indexing="xy"), -1).reshape(-1, 2)
+            args.energy = args.energy if args.energy != ap.get_default("energy") else 300.0
+            w = workloads.rough(pixels=pixels, per_pixel=args.per_pixel, energy=args.energy, pixel_streams=False)
         else:
             w = workloads.slab(n_primaries=args.pixels * args.pixels * args.per_pixel, energy=args.energy)
-        tri = os.path.join(d, "g.tri")
-        geometry.write_tri(tri, w.triangles)
         ms = []
         for sp in w.material_specs:
             p = os.path.join(d, sp.name + ".nmat")
             nmat.write(p, materials.build_raw_material(sp))
             ms.append(nb.Material.load(p))
-        g = nb.Geometry.from_tri_file(tri)
+        if args.workload == "rough":
+            g = nb.Geometry.from_triangles(nb.triangles_from_vertices(w.triangles), max_depth=12, split_count=16)
+        else:
+            tri = os.path.join(d, "g.tri")
+            geometry.write_tri(tri, w.triangles)
+            g = nb.Geometry.from_tri_file(tri)
         sim = nb.Simulation(g, ms, capacity=args.capacity, seed=args.seed, record_capacity=1 << 22,
                             block_size=args.block)
         runs = []
