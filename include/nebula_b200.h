@@ -5,7 +5,8 @@
  * and copies caller arrays during the call (the library owns all device
  * memory; the caller owns host arrays).  A simulation handle is bound to one
  * device and one CUDA stream; calls on one handle are not thread-safe,
- * distinct handles are independent.
+ * distinct handles are independent and may be driven from different host
+ * threads at the same time (graphs are captured in thread-local mode).
  *
  * Reference interfaces each group replaces (paths relative to the
  * reference's source/ directory):
