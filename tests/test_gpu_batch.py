@@ -34,12 +34,12 @@ def small_batch(tmp_path_factory):
     return geoms, mats, jobs
 
 
-def _plain_yields(geoms, mats, jobs):
+def _plain_yields(geoms, mats, jobs, physics=None):
     out = []
     for gi, seed, pri in jobs:
         g = geoms[gi]
         n_mat = 1 if gi == 0 else 2
-        sim = nb.Simulation(g, mats[:n_mat], capacity=1 << 14, seed=seed)
+        sim = nb.Simulation(g, mats[:n_mat], capacity=1 << 14, seed=seed, physics=physics)
         sim.push(pri)
         sim.run()
         rec = sim.flush_detected()
@@ -65,6 +65,23 @@ def test_batch_per_job_yields_equal_plain_runs(small_batch, block, thr, cap, gra
         assert c["primaries_started"] + c["spawned"] == c["detected"] + c["terminated"]
         assert c["queue_overflow"] == 0
     b.close()
+
+
+def test_batch_with_a_non_default_physics_selection(small_batch):
+    """The batched kernel compiled for run-time physics bits: per-job yields
+    equal plain runs with the same selection, and differ from the default
+    selection's."""
+    geoms, mats, jobs = small_batch
+    physics = {"interface_refraction": 0, "quantum_transmission": 0, "interface_absorption": 1,
+               "atomic_recoil_loss": 0}
+    ref = _plain_yields(geoms, mats, jobs, physics)
+    b = nb.Batch(geoms, mats, capacity=1 << 14, block_size=256, physics=physics)
+    b.set_jobs(jobs)
+    b.run()
+    se, bse = b.job_yields()
+    b.close()
+    assert np.array_equal(se, ref[:, 0]) and np.array_equal(bse, ref[:, 1])
+    assert not np.array_equal(ref, _plain_yields(geoms, mats, jobs))
 
 
 def test_batch_rejects_bad_job_ranges(small_batch):
