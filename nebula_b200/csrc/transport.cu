@@ -759,8 +759,8 @@ int batch_grid_size(int device, int block)
 	int sms = 148, per_sm = 0;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
 	// the cooperative grid must be co-resident for whichever instantiation runs
-	const void* kernels[] = { (const void*)k_batch<false>, (const void*)k_batch<true>,
-		(const void*)k_batch<false, PH_DEFAULT>, (const void*)k_batch<true, PH_DEFAULT> };
+	// (batches run without the adjoint: the host never sets it for them)
+	const void* kernels[] = { (const void*)k_batch<false>, (const void*)k_batch<false, PH_DEFAULT> };
 	for (const void* k : kernels) {
 		int n = 0;
 		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, block, 0);
@@ -772,9 +772,9 @@ int batch_grid_size(int device, int block)
 cudaError_t launch_batch(const StepParams& p, const BatchParams& b, int grid, int block, cudaStream_t s)
 {
 	void* args[] = { const_cast<StepParams*>(&p), const_cast<BatchParams*>(&b) };
-	const bool fixed = p.phys == PH_DEFAULT;
-	const void* k = p.adjoint ? (fixed ? (const void*)k_batch<true, PH_DEFAULT> : (const void*)k_batch<true>)
-		: (fixed ? (const void*)k_batch<false, PH_DEFAULT> : (const void*)k_batch<false>);
+	if (p.adjoint)
+		return cudaErrorInvalidValue;           // no batched adjoint
+	const void* k = p.phys == PH_DEFAULT ? (const void*)k_batch<false, PH_DEFAULT> : (const void*)k_batch<false>;
 	return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(block), args, 0, s);
 }
 

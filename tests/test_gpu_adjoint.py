@@ -156,3 +156,24 @@ def test_gradients_match_reference_driver_fd(tmp_path):
         se_fd = fd_pix.std(ddof=1) * np.sqrt(fd_pix.size) / N
         assert abs(adj - fd) <= 0.05 * abs(fd) + 3 * np.hypot(se_adj, se_fd), (str(ref["params"][k]), adj, fd, se_fd)
     prob.close()
+
+
+def test_adjoint_replay_with_energy_deposits(problem):
+    """Adjoint and energy deposits together (their own kernel
+    instantiation): with no work-function step the replay writes exactly the
+    forward run's deposit records and detected records."""
+    sims = []
+    for adj in (False, True):
+        s = nb.Simulation(problem.geometry, problem.materials, capacity=1 << 16, seed=21, tally=(16, 16),
+                          adjoint=adj, adjoint_w_step=0.0, deposit_capacity=1 << 22)
+        s.push(problem.primaries[:20000])
+        s.run()
+        sims.append(s)
+    key = lambda a, n: np.sort(a.view(np.dtype((np.void, n))).ravel()).tobytes()
+    dep = [s.drain_deposits() for s in sims]
+    det = [s.flush_detected() for s in sims]
+    assert len(dep[0]) > 20000
+    assert key(dep[0], 28) == key(dep[1], 28)
+    assert key(det[0], 36) == key(det[1], 36)
+    for s in sims:
+        s.close()
