@@ -7,9 +7,12 @@ times after one warm-up run, and prints one JSON line with the transport
 kernel time, primaries/s and events per primary.  ``--workload rough`` runs
 the 16 rough lines (1.2 M triangles, octree depth <= 12) on a ``pixels x
 pixels`` block at the centre of their 512 x 512 raster (300 eV unless
-``--energy`` is given); ``--workload slab`` the 1 um Si slab.  It is small enough for a
-full ncu capture of a few launches (``-k regex:k_step -s <n> -c <m>``) and
-keeps its whole state on one GPU.
+``--energy`` is given); ``--workload slab`` the 1 um Si slab; ``--workload
+batch`` the 64-job mixed batch, every job's primaries scaled by ``--scale``,
+in the batched persistent kernel (one launch per run; ``--block`` and
+``--capacity`` set its launch shape and pool).  It is small enough for a full
+ncu capture of a few launches (``-k regex:k_step -s <n> -c <m>``) and keeps
+its whole state on one GPU.
 """
 from __future__ import annotations
 
@@ -28,7 +31,8 @@ def main(argv=None):
     ap.add_argument("--capacity", type=int, default=1 << 18)
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--seed", type=int, default=3)
-    ap.add_argument("--workload", default="grating", choices=["grating", "slab", "rough"])
+    ap.add_argument("--workload", default="grating", choices=["grating", "slab", "rough", "batch"])
+    ap.add_argument("--scale", type=float, default=0.02, help="batch: fraction of every job's primaries")
     ap.add_argument("--block", type=int, default=0, help="threads per block of the step kernel (0: default)")
     args = ap.parse_args(argv)
 
@@ -36,6 +40,8 @@ def main(argv=None):
     import nebula_b200 as nb
     from nebula_b200.synth import workloads, geometry, materials, nmat
 
+    if args.workload == "batch":
+        return run_batch(args)
     with tempfile.TemporaryDirectory() as d:
         if args.workload == "grating":
             px = np.arange(128 - args.pixels // 2, 128 - args.pixels // 2 + args.pixels)
@@ -80,6 +86,29 @@ def main(argv=None):
                       "primaries": n, "kernel_ms": kms, "primaries_per_s": n / (kms / 1e3),
                       "events_per_primary": runs[-1][2] / n, "iterations": runs[-1][3],
                       "wall_s": float(np.mean([r[1] for r in runs]))}))
+
+
+def run_batch(args):
+    import numpy as np
+    import nebula_b200 as nb
+    from nebula_b200.tune_mixed_batch import load_mixed_batch
+
+    with tempfile.TemporaryDirectory() as d:
+        geoms, mats, jobs, _ = load_mixed_batch(d, scale=args.scale)
+        b = nb.Batch(geoms, mats, capacity=args.capacity, block_size=args.block or 512, refill_threshold=0.5)
+        b.set_jobs(jobs)
+        runs = []
+        for r in range(args.repeat + 1):
+            b.run()
+            if r > 0:
+                runs.append(b.kernel_ms())
+        c = b.counters()
+        b.close()
+    n = sum(len(p) for _, _, p in jobs)
+    kms = float(np.mean(runs))
+    print(json.dumps({"workload": "mixed batch x %g (%d jobs)" % (args.scale, len(jobs)), "primaries": n,
+                      "kernel_ms": kms, "primaries_per_s": n / (kms / 1e3),
+                      "events_per_primary": c["flights"] / n, "iterations": c["iterations"]}))
 
 
 if __name__ == "__main__":
