@@ -422,6 +422,9 @@ nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const* materials
 	nbl_counters* counters);
 
 /* ------------------------------------------------------------ debug entry points */
+/* The Philox4x32-10 bijection the transport draws its random numbers from
+ * (host evaluation of the same code): out = philox(counter, key). */
+nbl_status nbl_debug_philox(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4]);
 /* Table lookups on the device (which: 0 el_imfp 1 el_icdf 2 in_imfp 3 in_omega
  * 4 in_q 5 in_binding 6 ki_imfp 7 ki_w0 8 ki_binding) for n points;
  * `rounddown` selects get_rounddown. */

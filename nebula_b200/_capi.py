@@ -131,6 +131,7 @@ _DECLS = [
     ("nbl_sim_push_primaries", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("nbl_sim_push_primaries_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("nbl_sim_set_primary_offset", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("nbl_debug_philox", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("nbl_sim_step", C.c_int, [C.c_void_p, C.c_uint32, i64p]),
     ("nbl_sim_run", C.c_int, [C.c_void_p]),
     ("nbl_sim_drain_detected", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, i64p]),

@@ -4,6 +4,7 @@
 #include "device.hpp"
 
 #include <cuda_runtime.h>
+#include "../device/rng.cuh"
 #include <cmath>
 #include <cstring>
 #include <cstdio>
@@ -1146,6 +1147,19 @@ void nbl_sim_destroy(nbl_sim* s)
 }
 
 /* debug entry points */
+nbl_status nbl_debug_philox(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4])
+{
+	return guard([&] {
+		require(counter && key && out, "null argument");
+		uint32_t c[4] = { counter[0], counter[1], counter[2], counter[3] };
+		nbl::PhiloxKey k;
+		k.k0 = key[0];
+		k.k1 = key[1];
+		nbl::philox4x32_10(c, k);
+		for (int i = 0; i < 4; ++i) out[i] = c[i];
+	});
+}
+
 nbl_status nbl_debug_table_lookup(const nbl_material* m, int device, int32_t which, int32_t rounddown, int64_t n,
 	const float* x, const float* y, const float* z, float* out)
 {
