@@ -314,6 +314,21 @@ int run(int argc, char** argv)
 		return 1;
 	}
 	std::fprintf(stderr, "nebula_b200 (C ABI version %d): B200 electron transport\n\n", nbl_abi_version());
+	// the selected physics, as the reference's print_info lines report its
+	// compiled-in models (gpu_main.cu:239-243)
+	std::fprintf(stderr, "Physics models:\n");
+	if (cli.u64("inelastic-model") == 1)
+		std::fprintf(stderr, "  inelastic: kieft_inelastic (optical phonon loss %d, generate secondaries %d, "
+			"instantaneous momentum %d, momentum conservation %d)\n", (int)cli.flag("optical-phonon-loss"),
+			(int)cli.flag("generate-secondaries"), (int)cli.flag("instantaneous-momentum"),
+			(int)cli.flag("momentum-conservation"));
+	else
+		std::fprintf(stderr, "  inelastic: full_penn (generate secondaries %d)\n", (int)cli.flag("generate-secondaries"));
+	std::fprintf(stderr, "  elastic:   kieft_elastic (acoustic phonon loss %d, atomic recoil loss %d)\n",
+		(int)cli.flag("acoustic-phonon-loss"), (int)cli.flag("atomic-recoil-loss"));
+	std::fprintf(stderr, "  boundary:  boundary_intersect (quantum transmission %d, interface refraction %d, "
+		"interface absorption %d)\n\n", (int)cli.flag("quantum-transmission"), (int)cli.flag("interface-refraction"),
+		(int)cli.flag("interface-absorption"));
 	static char stdout_buffer[1 << 22];
 	std::setvbuf(stdout, stdout_buffer, _IOFBF, sizeof(stdout_buffer));
 

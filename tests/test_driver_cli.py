@@ -60,6 +60,9 @@ def test_usage_and_bad_arguments(driver, slab_files):
     # the slab needs material 0: none given
     r = _run([driver, tri, pri])
     assert r.returncode == 1 and r.stdout == b""
+    # the physics banner reports the selection (before any device call)
+    r = _run([driver, "--inelastic-model", "1", "--interface-absorption", "1", tri, pri, mat])
+    assert b"inelastic: kieft_inelastic" in r.stderr and b"interface absorption 1" in r.stderr
 
 
 def test_not_enough_materials(driver, tmp_path):
