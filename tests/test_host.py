@@ -104,6 +104,29 @@ def test_tri_loader_rejects_bad_rows(tmp_path):
     assert e.value.status == 7
 
 
+def test_pri_loader(tmp_path):
+    """nbl_load_pri_file: whole 36-byte records round-trip; a file whose size
+    is not a multiple of 36 is an IO error (load_pri_file.cpp:106-107); a
+    missing file too."""
+    import ctypes as C
+    from nebula_b200 import _capi
+    from nebula_b200.synth import primaries
+    rec = primaries.point_beam(5)
+    good = tmp_path / "good.pri"
+    primaries.write_pri(str(good), rec)
+    out = C.POINTER(_capi.Record)()
+    n = C.c_int64()
+    L = nb.lib()
+    assert L.nbl_load_pri_file(str(good).encode(), C.byref(out), C.byref(n)) == 0 and n.value == 5
+    got = np.frombuffer(C.string_at(out, 36 * n.value), dtype=nb.PRI_DTYPE)
+    L.nbl_free(out)
+    assert got.tobytes() == rec.tobytes()
+    bad = tmp_path / "bad.pri"
+    bad.write_bytes(rec.tobytes()[:-5])
+    assert L.nbl_load_pri_file(str(bad).encode(), C.byref(out), C.byref(n)) == 7
+    assert L.nbl_load_pri_file(b"/nonexistent/file.pri", C.byref(out), C.byref(n)) == 7
+
+
 def test_missing_material_file():
     with pytest.raises(nb.NblError) as e:
         nb.Material.load("/nonexistent/file.nmat")
