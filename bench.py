@@ -533,7 +533,7 @@ def rough_lines(args, dev, workdir):
         ms.append(nb.Material.load(pth))
     words = device_raster_scan(512, 512, 200, 0.5, 300.0, 40.0, 1.0, 11, dev)
     n = words.shape[0]
-    sim = nb.Simulation(g, ms, capacity=1 << 22, seed=31, record_capacity=1 << 24, tally=(512, 512), device=dev)
+    sim = nb.Simulation(g, ms, capacity=args.capacity, seed=31, record_capacity=1 << 24, tally=(512, 512), device=dev)
     pri_dev = words
     sim.reset()
     sim.push_device(pri_dev.data_ptr(), n)
@@ -569,7 +569,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--capacity", type=int, default=1 << 22)
+    ap.add_argument("--capacity", type=int, default=1 << 23)
     ap.add_argument("--record-capacity", type=int, default=1 << 24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the mixed-batch (batched vs plain) measurement")
