@@ -51,9 +51,10 @@ sys.path.insert(0, ROOT)
 METRIC = "primaries/s on 1 B200, plain vs batched; adjoint:forward time at yield err ≤3σ"
 BYTES_PER_EVENT = 96   # 48-byte electron state read + written per event
 # DRAM bytes (read + write) per event of the transport kernel on this workload,
-# from an ncu capture of one whole scan (dram__bytes_read.sum +
-# dram__bytes_write.sum over its 168 launches / its 1.4125e9 flights)
-DRAM_BYTES_PER_EVENT = 89.4
+# from an ncu capture of one whole scan at the default pool (2^23):
+# dram__bytes_read.sum + dram__bytes_write.sum over its 96 launches / its
+# 1.4125e9 flights
+DRAM_BYTES_PER_EVENT = 89.8
 
 
 def measured_peaks():
