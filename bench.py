@@ -534,7 +534,8 @@ def rough_lines(args, dev, workdir):
         ms.append(nb.Material.load(pth))
     words = device_raster_scan(512, 512, 200, 0.5, 300.0, 40.0, 1.0, 11, dev)
     n = words.shape[0]
-    sim = nb.Simulation(g, ms, capacity=args.capacity, seed=31, record_capacity=1 << 24, tally=(512, 512), device=dev)
+    sim = nb.Simulation(g, ms, capacity=args.capacity, seed=31, record_capacity=1 << 24, tally=(512, 512), device=dev,
+                        step_mode=args.step_mode)
     pri_dev = words
     sim.reset()
     sim.push_device(pri_dev.data_ptr(), n)
@@ -563,6 +564,86 @@ def rough_lines(args, dev, workdir):
             "octree_build_threads": os.cpu_count(), "mesh_generation_seconds": t_gen}
 
 
+# ---------------------------------------------------------------------------- profiling cases
+def run_case(args):
+    """A bounded run of one workload for profilers and timing sweeps
+    (``--case``): ``--repeat`` runs after one warm-up run, one JSON line with
+    the transport kernel time, primaries/s and events per primary.
+
+    grating: a ``--pixels`` x ``--pixels`` block at the centre of the 256 x 256
+             grating raster, ``--per-pixel`` primaries at ``--energy`` (500 eV);
+    rough:   the same block at the centre of the rough lines' 512 x 512 raster
+             (1.2 M triangles, octree depth <= 12; 300 eV unless given);
+    slab:    ``pixels^2 x per_pixel`` primaries on the 1 um Si slab;
+    batch:   the 64-job mixed batch with every job's primaries scaled by
+             ``--batch-scale``, in the batched persistent kernel.
+    Small enough for an ncu capture of a few launches on one GPU."""
+    import nebula_b200 as nb
+    from nebula_b200.synth import workloads, geometry, materials, nmat
+    if args.case == "batch":
+        from nebula_b200.tune_mixed_batch import load_mixed_batch
+        with tempfile.TemporaryDirectory() as d:
+            geoms, mats, jobs, _ = load_mixed_batch(d, scale=args.batch_scale)
+            b = nb.Batch(geoms, mats, capacity=args.capacity, block_size=args.block or 512, refill_threshold=0.5)
+            b.set_jobs(jobs)
+            runs = []
+            for r in range(args.repeat + 1):
+                b.run()
+                if r > 0:
+                    runs.append(b.kernel_ms())
+            c = b.counters()
+            b.close()
+        n = sum(len(p) for _, _, p in jobs)
+        kms = float(np.mean(runs))
+        print(json.dumps({"case": "mixed batch x %g (%d jobs)" % (args.batch_scale, len(jobs)), "primaries": n,
+                          "kernel_ms": kms, "primaries_per_s": n / (kms / 1e3),
+                          "events_per_primary": c["flights"] / n, "iterations": c["iterations"]}))
+        return
+    energy = args.energy if args.energy else (300.0 if args.case == "rough" else 500.0)
+    with tempfile.TemporaryDirectory() as d:
+        if args.case == "grating":
+            px = np.arange(128 - args.pixels // 2, 128 - args.pixels // 2 + args.pixels)
+            pixels = np.stack(np.meshgrid(px, px, indexing="xy"), -1).reshape(-1, 2)
+            w = workloads.grating(pixels=pixels, per_pixel=args.per_pixel, energy=energy)
+        elif args.case == "rough":
+            px = np.arange(256 - args.pixels // 2, 256 - args.pixels // 2 + args.pixels)
+            pixels = np.stack(np.meshgrid(px, px, indexing="xy"), -1).reshape(-1, 2)
+            w = workloads.rough(pixels=pixels, per_pixel=args.per_pixel, energy=energy, pixel_streams=False)
+        else:
+            w = workloads.slab(n_primaries=args.pixels * args.pixels * args.per_pixel, energy=energy)
+        ms = []
+        for sp in w.material_specs:
+            p = os.path.join(d, sp.name + ".nmat")
+            nmat.write(p, materials.build_raw_material(sp))
+            ms.append(nb.Material.load(p))
+        if args.case == "rough":
+            g = nb.Geometry.from_triangles(nb.triangles_from_vertices(w.triangles), max_depth=12, split_count=16)
+        else:
+            tri = os.path.join(d, "g.tri")
+            geometry.write_tri(tri, w.triangles)
+            g = nb.Geometry.from_tri_file(tri)
+        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=3, record_capacity=1 << 22, block_size=args.block,
+                            step_mode=args.step_mode)
+        runs = []
+        for r in range(args.repeat + 1):
+            sim.reset()
+            sim.push(w.primaries)
+            t0 = time.perf_counter()
+            sim.run()
+            wall = time.perf_counter() - t0
+            c = sim.counters()
+            sim.flush_detected()
+            if r > 0:
+                runs.append((sim.kernel_ms(), wall, c["flights"], c["iterations"]))
+        sim.close()
+    n = len(w.primaries)
+    kms = float(np.mean([r[0] for r in runs]))
+    print(json.dumps({"case": "%s %dx%dx%d at %g eV" % (args.case, args.pixels, args.pixels, args.per_pixel, energy),
+                      "primaries": n, "capacity": args.capacity, "step_mode": args.step_mode, "kernel_ms": kms,
+                      "primaries_per_s": n / (kms / 1e3), "events_per_primary": runs[-1][2] / n,
+                      "iterations": runs[-1][3], "wall_s": float(np.mean([r[1] for r in runs]))}))
+
+
 # ---------------------------------------------------------------------------- GPU
 def main():
     ap = argparse.ArgumentParser()
@@ -578,9 +659,21 @@ def main():
     ap.add_argument("--no-rough", action="store_true", help="skip the large-mesh (rough lines) measurement")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own GPU driver beside its CPU driver")
+    ap.add_argument("--case", choices=["grating", "rough", "slab", "batch"],
+                    help="run one bounded profiling case instead of the benchmark (see run_case)")
+    ap.add_argument("--pixels", type=int, default=64, help="--case: pixels per side of the scanned block")
+    ap.add_argument("--per-pixel", type=int, default=100, help="--case: primaries per pixel")
+    ap.add_argument("--energy", type=float, default=0.0, help="--case: beam energy in eV (0: the case's own)")
+    ap.add_argument("--repeat", type=int, default=1, help="--case: timed runs after one warm-up run")
+    ap.add_argument("--batch-scale", type=float, default=0.02, help="--case batch: fraction of every job's primaries")
+    ap.add_argument("--block", type=int, default=0, help="--case: threads per block of the kernel (0: default)")
+    ap.add_argument("--step-mode", type=int, default=0, choices=[0, 1],
+                    help="wavefront iterations: 0 split (an item interacts or flies), 1 fused")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.case:
+        return run_case(args)
 
     import torch
     import nebula_b200 as nb
@@ -606,7 +699,7 @@ def main():
         from nebula_b200 import replicas
         sim = nb.Simulation(g, ms, capacity=args.capacity, seed=replicas.replica_seed(1000, rank), device=dev,
                             tally=w.n_pixels,
-                            stream=stream.cuda_stream, record_capacity=args.record_capacity)
+                            stream=stream.cuda_stream, record_capacity=args.record_capacity, step_mode=args.step_mode)
         pri_dev = torch.from_numpy(w.primaries.view(np.uint8)).to(f"cuda:{dev}")
         pri_host = torch.from_numpy(w.primaries.view(np.uint8).copy()).pin_memory()
         rec_host = torch.empty(args.record_capacity * 36, dtype=torch.uint8).pin_memory()

@@ -235,6 +235,8 @@ typedef struct nbl_params {
 	uint32_t deposit_capacity;   /* deposit records buffered on the device; 0: no records */
 	nbl_deposit_grid deposit_grid; /* voxel grid of the losses; n = 0: none */
 	nbl_image_filter image_filter; /* detector acceptance of the per-pixel images */
+	int32_t step_mode;           /* 0: split wavefront (an iteration's item either interacts or flies);
+	                                1: fused (interaction and the next flight in one item); same results */
 } nbl_params;
 void nbl_params_defaults(nbl_params* p);
 
@@ -407,10 +409,17 @@ void nbl_batch_destroy(nbl_batch* b);
  *   outputs: detected records (device, records_cap of them) and their count,
  *            optional per-pixel SE/BSE images (tally_nx x tally_ny, device) and
  *            histogram (hist_bins, device), all cleared first; counters (host)
+ * The image filter (detector acceptance) applies as in nbl_sim_create.
  * Limits: capacity <= NBL_NOALLOC_MAX_CAPACITY (0 selects it), at most
  * NBL_NOALLOC_MAX_MATERIALS materials, geometry <= 2 MiB and tables <= 4 MiB
- * in device layout, no adjoint; larger inputs are rejected.  The first call on
- * a device looks up the array's address; make it before any stream capture.
+ * in device layout, no adjoint, no energy deposits (deposit_capacity and
+ * deposit_grid must be zero); other requests are rejected.  The first call on
+ * a device looks up the array's address and keeps it for the process; make it
+ * before any stream capture, and make no call on a device after resetting it
+ * (cudaDeviceReset).  With CUDA's default lazy module loading the array is
+ * reserved at the first call on a device, not when the library is loaded:
+ * make one call before giving the device to another allocator.  A call waits
+ * on its stream and returns when the run is complete.
  * Calls share the array and it keeps the previous call's contents: each call
  * clears what must start at zero, and calls that overlap on the GPU race. */
 #define NBL_NOALLOC_MAX_CAPACITY 2048
@@ -422,6 +431,9 @@ nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const* materials
 	nbl_counters* counters);
 
 /* ------------------------------------------------------------ debug entry points */
+/* Architecture the transport kernel was loaded for on `device`, as the CUDA
+ * runtime reports it (cudaFuncAttributes::binaryVersion: 100 = sm_100). */
+nbl_status nbl_debug_kernel_arch(int device, int32_t* binary_version);
 /* The Philox4x32-10 bijection the transport draws its random numbers from
  * (host evaluation of the same code): out = philox(counter, key). */
 nbl_status nbl_debug_philox(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4]);

@@ -80,7 +80,7 @@ class Params(C.Structure):
                 ("hist_emax", C.c_float), ("max_events", C.c_uint32), ("stream", C.c_void_p),
                 ("physics", PhysicsOpts), ("adjoint", C.c_int32), ("adjoint_w_step", C.c_float),
                 ("deposit_capacity", C.c_uint32), ("deposit_grid", DepositGrid),
-                ("image_filter", ImageFilter)]
+                ("image_filter", ImageFilter), ("step_mode", C.c_int32)]
 
 
 class BatchJob(C.Structure):
@@ -131,6 +131,7 @@ _DECLS = [
     ("nbl_sim_push_primaries", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("nbl_sim_push_primaries_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("nbl_sim_set_primary_offset", C.c_int, [C.c_void_p, C.c_uint64]),
+    ("nbl_debug_kernel_arch", C.c_int, [C.c_int, C.POINTER(C.c_int32)]),
     ("nbl_debug_philox", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     ("nbl_sim_step", C.c_int, [C.c_void_p, C.c_uint32, i64p]),
     ("nbl_sim_run", C.c_int, [C.c_void_p]),

@@ -635,7 +635,6 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		require(cap >= 32 && cap <= (1u << 28), "capacity must be 32..2^28");
 		s->block = params->block_size ? (int)params->block_size : 256;
 		require(s->block % 32 == 0 && s->block >= 32 && s->block <= 256, "block_size must be a multiple of 32 in 32..256");
-		s->grid = params->grid_size ? (int)params->grid_size : step_grid_size(s->device, s->block);
 		uint32_t gi = params->iterations_per_graph ? params->iterations_per_graph : 24;
 		gi = (gi + 5) / 6 * 6;
 		s->graph_iters = gi;
@@ -774,6 +773,9 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		sp.max_events = params->max_events ? params->max_events : (1u << 22);
 		require(sp.max_events < (1u << 24), "max_events must be < 2^24");
 		sp.adjoint = adj ? 1 : 0;
+		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (split) or 1 (fused)");
+		sp.split = params->step_mode == 0 ? 1 : 0;
+		s->grid = params->grid_size ? (int)params->grid_size : step_grid_size(s->device, s->block, sp);
 		s->ensure_primary_capacity(1024);
 		sp.n_primaries = 0;
 		s->reset_device_state();
@@ -843,9 +845,9 @@ nbl_status nbl_sim_run(nbl_sim* s)
 		require(s != nullptr, "null simulation");
 		set_device(s->device);
 		// the budget bounds the iterations: an electron cannot outlive
-		// max_events flights, and the pool refills at least one primary per
-		// iteration while primaries are left
-		const uint64_t bound = (uint64_t)s->sp.max_events + s->n_pri + 16;
+		// max_events flights (two iterations each when split), and the pool
+		// refills at least one primary per iteration while primaries are left
+		const uint64_t bound = 2ull * s->sp.max_events + s->n_pri + 16;
 		const uint64_t max_graphs = bound / s->graph_iters + 2;
 		const int64_t left = s->advance(max_graphs);
 		s->check_errors();
@@ -1147,6 +1149,17 @@ void nbl_sim_destroy(nbl_sim* s)
 }
 
 /* debug entry points */
+nbl_status nbl_debug_kernel_arch(int device, int32_t* binary_version)
+{
+	return guard([&] {
+		require(binary_version != nullptr, "null argument");
+		set_device(device);
+		int v = 0;
+		CU(step_binary_version(device, &v));
+		*binary_version = v;
+	});
+}
+
 nbl_status nbl_debug_philox(const uint32_t counter[4], const uint32_t key[2], uint32_t out[4])
 {
 	return guard([&] {

@@ -85,6 +85,7 @@ struct StepParams {
 	double* grid;             // eV per voxel [gn[2]][gn[1]][gn[0]]
 	float g_org[3], g_inv[3]; // grid origin, 1 / voxel size
 	int32_t gn[3];
+	int32_t split;            // 1: split iterations (an item interacts or flies), 0: fused
 };
 
 // Work-function sign of a primary for material m (0 or 1): +1 or -1 from a
@@ -132,7 +133,10 @@ cudaError_t launch_event_kat(const DevGeometry& g, const DevMaterial* mats, uint
 	float* state_out, int32_t* mat_out, int32_t* status, float* se_out, int32_t* has_se, int32_t* used,
 	cudaStream_t s);
 cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s);
-int step_grid_size(int device, int block);
+// blocks for `block` threads at full occupancy of the step kernel that `p` selects
+int step_grid_size(int device, int block, const StepParams& p);
+// binary architecture (major * 10 + minor) of the loaded transport kernel
+cudaError_t step_binary_version(int device, int* version);
 cudaError_t launch_batch(const StepParams& p, const BatchParams& b, int grid, int block, cudaStream_t s);
 int batch_grid_size(int device, int block);
 

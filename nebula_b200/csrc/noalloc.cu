@@ -14,12 +14,21 @@
 //
 // Limits (rejected with NBL_ERR_INVALID_ARG beyond them): capacity at most
 // NBL_NOALLOC_MAX_CAPACITY electrons, at most NBL_NOALLOC_MAX_MATERIALS
-// materials, geometry and tables within the byte budgets below.  The first
-// call on a device looks the array's device address up
-// (cudaGetSymbolAddress), so make that first call before any stream capture.
-// All calls share the one array and it keeps the previous call's contents:
-// each call clears the parts that must start at zero, and two calls whose
-// work overlaps on the GPU (different streams, different threads) race on it.
+// materials, geometry and tables within the byte budgets below, no adjoint,
+// no energy deposits.  The first call on a device looks the array's device
+// address up (cudaGetSymbolAddress) and keeps it for the life of the process,
+// so make that first call before any stream capture, and make no call on a
+// device after the caller has reset it (cudaDeviceReset): the kept address
+// belongs to the context that the reset destroyed.  Under CUDA's default lazy
+// module loading the array is reserved when the library's kernels are first
+// used on a device, not when the library is loaded: a caller that hands the
+// device to its own allocator afterwards should make one call first (or load
+// modules eagerly, CUDA_MODULE_LOADING=EAGER).  A call waits on its stream:
+// it reads the run's progress from the device between rounds of iterations
+// and returns when the run is complete.  All calls share the one array and it
+// keeps the previous call's contents: each call clears the parts that must
+// start at zero, and two calls whose work overlaps on the GPU (different
+// streams, different threads) race on it.
 #include <cuda_runtime.h>
 #include <cstring>
 #include <mutex>
@@ -110,6 +119,12 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		require(n_materials >= 1 && n_materials <= NBL_NOALLOC_MAX_MATERIALS,
 			"nbl_run_noalloc: at most " + std::to_string(NBL_NOALLOC_MAX_MATERIALS) + " materials");
 		require(params->adjoint == 0, "nbl_run_noalloc: the adjoint is not available without allocation");
+		const nbl_deposit_grid& dgp = params->deposit_grid;
+		require(params->deposit_capacity == 0 && dgp.n[0] == 0 && dgp.n[1] == 0 && dgp.n[2] == 0,
+			"nbl_run_noalloc: energy deposits are not available without allocation");
+		const nbl_image_filter& flt = params->image_filter;
+		require(!flt.enabled || (flt.cos_min <= flt.cos_max && flt.cos_min >= -1.0f && flt.cos_max <= 1.0f),
+			"image filter needs -1 <= cos_min <= cos_max <= 1");
 		const uint32_t phys = physics_bits(params->physics);
 		const bool kieft = (phys & PH_KIEFT) != 0;
 		const uint32_t cap = params->capacity ? params->capacity : NA_CAPACITY;
@@ -242,6 +257,10 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		sp.tal.nx = nx; sp.tal.ny = ny;
 		sp.tal.n_bins = n_bins;
 		sp.tal.hist_emax = params->hist_emax > 0 ? params->hist_emax : 1000.0f;
+		// detector acceptance of the images, as nbl_sim_create applies it
+		sp.tal.filter = flt.enabled ? 1 : 0;
+		sp.tal.cos_min = flt.enabled ? flt.cos_min : 0.0f;
+		sp.tal.cos_max = flt.enabled ? flt.cos_max : 0.0f;
 		sp.counters = reinterpret_cast<unsigned long long*>(base + OFF_COUNTERS);
 		sp.max_events = params->max_events ? params->max_events : (1u << 22);
 		require(sp.max_events < (1u << 24), "max_events must be < 2^24");
@@ -249,14 +268,17 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 
 		const int block = params->block_size ? (int)params->block_size : 256;
 		require(block % 32 == 0 && block >= 32 && block <= 256, "block_size must be a multiple of 32 in 32..256");
-		const int grid = params->grid_size ? (int)params->grid_size : step_grid_size(params->device, block);
+		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (split) or 1 (fused)");
+		sp.split = params->step_mode == 0 ? 1 : 0;
+		const int grid = params->grid_size ? (int)params->grid_size : step_grid_size(params->device, block, sp);
 		const uint32_t check_every = 24;
-		const uint64_t bound = (uint64_t)sp.max_events + (uint64_t)n_primaries + 64;
+		const uint64_t bound = 2ull * sp.max_events + (uint64_t)n_primaries + 64;
 		uint32_t ctrl[SLOT_WORDS];
 		unsigned long long flights = 0, last_flights = ~0ull;
 		int stalled = 0;
 		bool done = false;
-		for (uint64_t it = 0; it < bound && !done; ) {
+		uint64_t it = 0;
+		for (; it < bound && !done; ) {
 			for (uint32_t k = 0; k < check_every; ++k, ++it)
 				cuda_ok(launch_step(sp, (uint32_t)(it % 6), grid, block, s), "transport launch");
 			const uint32_t slot = (uint32_t)(it % 3);
@@ -292,6 +314,7 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 			counters->queue_overflow = c[CNT_QUEUE_OVERFLOW]; counters->record_overflow = c[CNT_RECORD_OVERFLOW];
 			counters->event_budget = c[CNT_EVENT_BUDGET]; counters->spilled = c[CNT_SPILLED];
 			counters->primaries_total = (uint64_t)n_primaries;
+			counters->iterations = it;
 			counters->records_pending = *n_records;
 		}
 		if (c[CNT_QUEUE_OVERFLOW] || c[CNT_RECORD_OVERFLOW] || ndet > records_cap)

@@ -254,6 +254,34 @@ __device__ __forceinline__ int free_flight(const StepParams& P, const RunView& r
 	return -1;
 }
 
+// Whether the free flight of an electron that survived its interaction gets
+// past the checks at the top of free_flight's first hop (state only, no
+// random draw): a split iteration makes the decision at the interaction, so
+// that only electrons that will walk are queued for a flight.  Counts what
+// free_flight would count for an electron that stops there.
+template<bool ADJ>
+__device__ __forceinline__ bool flight_starts(const StepParams& P, const RunView& rv, const Electron& p, int mat,
+	uint32_t event, LocalCounters& lc, const float* dbar)
+{
+	bool go = true;
+	if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) {
+		lc.add(CNT_NAN);
+		go = false;
+	} else if (!in_domain(*rv.geom, p.pos.x, p.pos.y, p.pos.z)) {
+		go = false;
+	} else if (event >= P.max_events) {
+		lc.add(CNT_EVENT_BUDGET);
+		go = false;
+	} else if (mat >= 0) {
+		const DevMaterial* m = P.mats + mat;
+		const float barrier = (ADJ && dbar && mat < 2) ? fa(m->barrier, dbar[mat]) : m->barrier;
+		go = !(p.E < fa(barrier, P.energy_threshold));
+	}
+	if (!go)
+		lc.add(CNT_FLIGHTS);
+	return go;
+}
+
 __device__ __forceinline__ void store_electron(const Queue& q, uint32_t slot, const Electron& p, int mat, int last_tri,
 	uint32_t tag, uint32_t event, uint64_t lineage)
 {
@@ -332,7 +360,17 @@ __device__ __forceinline__ void deposit(const StepParams& P, bool scat, const El
 		lc.add(CNT_DEPOSITS);
 }
 
-template<bool ADJ, bool BATCH, bool DEP = false, uint32_t PHC = 0u>
+// SPLIT: an item either interacts or flies, never both.  Items of the
+// boundary / elastic / inelastic queues perform their interaction and, if the
+// electron goes on, queue it in the flight queue (EV_NEW) of the next
+// iteration; items of the flight queue, the drained ring and the new
+// primaries perform a free flight and queue the electron for the event it
+// ends in.  Every lane of a flight-segment warp then walks the octree (the
+// electrons that end at their interaction -- detected, absorbed, below the
+// escape cut -- no longer idle their lanes through the walks of the others),
+// at the price of an extra queue pass per event.  Each electron's sequence
+// of events and random numbers is the same either way.
+template<bool ADJ, bool BATCH, bool DEP = false, uint32_t PHC = 0u, bool SPLIT = false>
 __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc,
 	float* s_lane = nullptr)
 {
@@ -611,15 +649,20 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			}
 		}
 
-		// next free flight
+		// next free flight (SPLIT: the flight queue, for electrons that
+		// interacted in this item)
 		int qtype = -1;
-		if (status == ST_RUNNING)
-			qtype = free_flight<ADJ>(P, rv, p, mat, last_tri, event, stream_tag, lineage, sc, lc,
-				wshift ? dbar : nullptr);
+		if (status == ST_RUNNING) {
+			if (SPLIT && kind < EV_NEW)
+				qtype = flight_starts<ADJ>(P, rv, p, mat, event, lc, wshift ? dbar : nullptr) ? EV_NEW : -1;
+			else
+				qtype = free_flight<ADJ>(P, rv, p, mat, last_tri, event, stream_tag, lineage, sc, lc,
+					wshift ? dbar : nullptr);
+		}
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
 			lc.add(CNT_TERMINATED);
 #pragma unroll
-		for (int t = 0; t < 3; ++t) {
+		for (int t = 0; t < (SPLIT ? 4 : 3); ++t) {
 			const bool mine = qtype == t;
 			const uint32_t slot = warp_reserve(cw + t, mine);
 			if (mine) {
@@ -654,7 +697,7 @@ __device__ __forceinline__ void flush_counters(const StepParams& P, uint32_t* s_
 // DEP: energy deposits on (a separate instantiation, so the plain step keeps
 // none of their code).  PHC: nonzero = the physics selection fixed at
 // compile time (PH_DEFAULT only).
-template<bool ADJ, bool DEP, uint32_t PHC = 0u>
+template<bool ADJ, bool DEP, uint32_t PHC = 0u, bool SPLIT = false>
 __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
@@ -664,7 +707,7 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 	__syncthreads();
 	LocalCounters lc{ s_counters };
 	const BatchParams none{};
-	step_iteration<ADJ, false, DEP, PHC>(P, none, it, lc, s_lane);
+	step_iteration<ADJ, false, DEP, PHC, SPLIT>(P, none, it, lc, s_lane);
 	flush_counters(P, s_counters);
 }
 
@@ -728,30 +771,55 @@ __global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const Batc
 	flush_counters(P, s_counters);
 }
 
-cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)
+// The step kernel instantiation a run's parameters select: adjoint or not,
+// deposits or not, the default physics selection fixed at compile time or the
+// run-time word, split or fused iterations.
+template<bool SPLIT>
+static const void* step_kernel_for(const StepParams& p)
 {
 	const bool dep = p.dep || p.grid;
 	const bool fixed = p.phys == PH_DEFAULT;
 	if (p.adjoint) {
-		if (dep) k_step<true, true><<<grid, block, 0, s>>>(p, iteration);
-		else if (fixed) k_step<true, false, PH_DEFAULT><<<grid, block, 0, s>>>(p, iteration);
-		else k_step<true, false><<<grid, block, 0, s>>>(p, iteration);
-	} else {
-		if (dep) k_step<false, true><<<grid, block, 0, s>>>(p, iteration);
-		else if (fixed) k_step<false, false, PH_DEFAULT><<<grid, block, 0, s>>>(p, iteration);
-		else k_step<false, false><<<grid, block, 0, s>>>(p, iteration);
+		if (dep) return (const void*)k_step<true, true, 0u, SPLIT>;
+		if (fixed) return (const void*)k_step<true, false, PH_DEFAULT, SPLIT>;
+		return (const void*)k_step<true, false, 0u, SPLIT>;
 	}
-	return cudaGetLastError();
+	if (dep) return (const void*)k_step<false, true, 0u, SPLIT>;
+	if (fixed) return (const void*)k_step<false, false, PH_DEFAULT, SPLIT>;
+	return (const void*)k_step<false, false, 0u, SPLIT>;
 }
 
-int step_grid_size(int device, int block)
+static const void* step_kernel(const StepParams& p)
+{
+	return p.split ? step_kernel_for<true>(p) : step_kernel_for<false>(p);
+}
+
+cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)
+{
+	void* args[] = { const_cast<StepParams*>(&p), &iteration };
+	return cudaLaunchKernel(step_kernel(p), dim3(grid), dim3(block), args, 0, s);
+}
+
+int step_grid_size(int device, int block, const StepParams& p)
 {
 	int sms = 148, per_sm = 1;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step<false, false>, block, 0);
+	// occupancy of the instantiation these parameters launch
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel(p), block, 0);
 	if (per_sm < 1)
 		per_sm = 1;
 	return sms * per_sm;
+}
+
+cudaError_t step_binary_version(int device, int* version)
+{
+	cudaError_t e = cudaSetDevice(device);
+	if (e != cudaSuccess)
+		return e;
+	cudaFuncAttributes a{};
+	e = cudaFuncGetAttributes(&a, k_step<false, false, PH_DEFAULT>);
+	*version = a.binaryVersion;
+	return e;
 }
 
 int batch_grid_size(int device, int block)

@@ -254,3 +254,12 @@ def test_resumed_and_sharded_scans_give_the_whole_scans_records(inputs):
     sim.run()
     assert _sorted(sim.flush_detected()) != _sorted(resumed[1])
     sim.close()
+
+
+def test_loaded_transport_kernel_is_sm100():
+    # the runtime's own report of the loaded kernel image: built for sm_100
+    import ctypes as C
+    from nebula_b200 import _capi
+    v = C.c_int32()
+    _capi.check(_capi.lib().nbl_debug_kernel_arch(0, C.byref(v)))
+    assert v.value == 100, v.value

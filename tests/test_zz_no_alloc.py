@@ -31,7 +31,8 @@ def _inputs(tmp_path):
     return nb.Geometry.from_tri_file(tri), nb.Material.load(mat), pri
 
 
-def _run_noalloc(g, m, pri, seed, capacity=2048, tally=(8, 4), records_cap=1 << 16):
+def _run_noalloc(g, m, pri, seed, capacity=2048, tally=(8, 4), records_cap=1 << 16, cos_range=None,
+                 deposit_capacity=0):
     import torch
     dev = torch.device("cuda:0")
     d_pri = torch.from_numpy(pri.view(np.uint8).copy()).to(dev)
@@ -47,6 +48,10 @@ def _run_noalloc(g, m, pri, seed, capacity=2048, tally=(8, 4), records_cap=1 << 
     p.tally_nx, p.tally_ny = tally
     p.hist_bins = 200
     p.hist_emax = 1000.0
+    if cos_range is not None:
+        p.image_filter.enabled = 1
+        p.image_filter.cos_min, p.image_filter.cos_max = cos_range
+    p.deposit_capacity = deposit_capacity
     mats = (C.c_void_p * 1)(m._h.value if isinstance(m._h, C.c_void_p) else m._h)
     n = C.c_int64()
     cnt = _capi.Counters()
@@ -60,8 +65,9 @@ def _run_noalloc(g, m, pri, seed, capacity=2048, tally=(8, 4), records_cap=1 << 
             d_hist.cpu().numpy(), {k: int(getattr(cnt, k)) for k in _capi.COUNTER_NAMES})
 
 
-def _run_allocating(g, m, pri, seed, tally=(8, 4)):
-    sim = nb.Simulation(g, [m], capacity=2048, seed=seed, tally=tally, hist_bins=200, hist_emax=1000.0)
+def _run_allocating(g, m, pri, seed, tally=(8, 4), cos_range=None):
+    sim = nb.Simulation(g, [m], capacity=2048, seed=seed, tally=tally, hist_bins=200, hist_emax=1000.0,
+                        image_cos_range=cos_range)
     sim.push(pri)
     sim.run()
     rec = sim.flush_detected()
@@ -89,6 +95,19 @@ def test_noalloc_matches_allocating_run_twice(tmp_path):
         for k in ("flights", "boundary", "elastic", "inelastic", "spawned", "detected", "terminated",
                   "primaries_started"):
             assert c[k] == ref[4][k], k
+        assert c["iterations"] > 0 and c["iterations"] % 24 == 0
+
+
+def test_noalloc_applies_the_image_filter(tmp_path):
+    # detector acceptance cone: the images count only detections within 60
+    # degrees of +z, as the allocating run does; the records stay unfiltered
+    g, m, pri = _inputs(tmp_path)
+    ref = _run_allocating(g, m, pri, seed=5, cos_range=(0.5, 1.0))
+    full = _run_allocating(g, m, pri, seed=5)
+    rec, se, bse, _, _ = _run_noalloc(g, m, pri, seed=5, cos_range=(0.5, 1.0))
+    assert _sorted(rec) == _sorted(ref[0])
+    assert np.array_equal(se.astype(np.uint32), ref[1]) and np.array_equal(bse.astype(np.uint32), ref[2])
+    assert se.sum() + bse.sum() < full[1].sum() + full[2].sum()
 
 
 def test_noalloc_rejects_oversize_requests(tmp_path):
@@ -96,3 +115,6 @@ def test_noalloc_rejects_oversize_requests(tmp_path):
     with pytest.raises(nb.NblError) as e:
         _run_noalloc(g, m, pri, seed=1, capacity=4096)
     assert e.value.status == 1 and "capacity" in str(e.value)
+    with pytest.raises(nb.NblError) as e:
+        _run_noalloc(g, m, pri, seed=1, deposit_capacity=1024)
+    assert e.value.status == 1 and "deposits" in str(e.value)
