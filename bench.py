@@ -337,9 +337,18 @@ def reference_arm(args):
 # ---------------------------------------------------------------------------- batch
 def batched_vs_plain(args, dev, workdir):
     """The mixed 64-job batch: one persistent batched launch against the
-    plain wavefront run job by job (one pool reused per geometry, with the
+    plain wavefront run job after job (one pool reused per geometry, with the
     plain bench's capacity; pool creation not timed), same seeds, so per-job
-    yields must be identical.
+    records must be identical.  Both arms deliver the same outputs -- every
+    job's detected 36-byte records on the host -- and are timed two ways:
+
+    device: the transport kernels alone (CUDA events around the batched
+            launch; around every graph of the plain runs, summed);
+    e2e:    wall time from the host primaries to the host records (batched:
+            upload of the batch's primaries and job table, the launch, the
+            records' read-back; plain: per job the push, the run and the
+            drain of its records).
+
     Batch parameters come from the autotuner's stored choice when present."""
     import torch
     import nebula_b200 as nb
@@ -354,19 +363,32 @@ def batched_vs_plain(args, dev, workdir):
     else:
         params = dict(capacity=1 << 22, block=512, threshold=0.5, source="default")
     b = nb.Batch(geoms, mats, capacity=params["capacity"], block_size=params["block"],
-                 refill_threshold=params["threshold"], device=dev)
-    b.set_jobs(jobs)
-    b.run()                                     # warm-up
-    batch_ms = []
-    for _ in range(args.steps):
+                 refill_threshold=params["threshold"], device=dev, record_capacity=1 << 24)
+
+    # the batch's primaries laid end to end, as the caller holds them (the
+    # plain arm holds one array per job)
+    all_pri = np.ascontiguousarray(np.concatenate([p for _, _, p in jobs]), nb.PRI_DTYPE)
+
+    def batch_pass():
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        b.set_jobs(jobs, primaries=all_pri)
         b.run()
-        batch_ms.append(b.kernel_ms())
+        rec, job = b.records()                  # every job's records and their job ids, on the host
+        return (rec, job), time.perf_counter() - t0, b.kernel_ms()
+
+    batch_pass()                                # warm-up
+    b_wall, b_dev = [], []
+    for _ in range(args.steps):
+        _, w, m = batch_pass()
+        b_wall.append(w)
+        b_dev.append(m)
     c = b.counters()
-    se_b, bse_b = b.job_yields()
+    recs_b = b.job_records()
     b.close()
 
     def plain_pass():
-        se, ms_dev, wall = [], 0.0, 0.0
+        recs, ms_dev, wall, flights = [], 0.0, 0.0, 0
         cur = None
         for gi, seed, pri in jobs:
             if cur is None or cur[0] != gi:
@@ -384,25 +406,35 @@ def batched_vs_plain(args, dev, workdir):
             rec = s.flush_detected()
             wall += time.perf_counter() - t0
             ms_dev += s.kernel_ms()
-            se.append(int((rec["E"] < 50).sum()))
+            flights += s.counters()["flights"]
+            recs.append(rec)
         cur[1].close()
-        return np.array(se), wall, ms_dev
+        return recs, wall, ms_dev, flights
 
     plain_pass()                                # warm-up
-    walls, devs = [], []
+    p_wall, p_dev = [], []
     for _ in range(args.steps):
-        se_p, w, m = plain_pass()
-        walls.append(w)
-        devs.append(m)
-    bm = float(np.mean(batch_ms)) / 1e3
-    pw = float(np.mean(walls))
+        recs_p, w, m, p_flights = plain_pass()
+        p_wall.append(w)
+        p_dev.append(m)
+    srt = lambda r: np.sort(r.view(np.dtype((np.void, 36))).ravel()).tobytes()
+    identical = all(len(x) == len(y) and srt(x) == srt(y) for x, y in zip(recs_b, recs_p))
+    bd, pd = float(np.mean(b_dev)) / 1e3, float(np.mean(p_dev)) / 1e3
+    bw, pw = float(np.mean(b_wall)), float(np.mean(p_wall))
     return {"workload": "mixed batch: %d jobs, %d primaries (slab / gratings pitch 20-64 nm, 200 eV-20 keV, "
                         "1e3-1e6 primaries per job)" % (len(jobs), n_pri),
-            "value": n_pri / bm, "unit": "primaries/s", "seconds": bm,
-            "plain_value": n_pri / pw, "plain_seconds": pw, "plain_transport_seconds": float(np.mean(devs)) / 1e3,
-            "ratio_batched_over_plain": pw / bm, "flights": c["flights"], "iterations": c["iterations"],
-            "spilled": c["spilled"], "per_job_yields_identical": bool(np.array_equal(se_b, se_p)),
-            "se_total": int(np.sum(se_b)), "bse_total": int(np.sum(bse_b)),
+            "value": n_pri / bd, "unit": "primaries/s", "seconds": bd,
+            "plain_value": n_pri / pd, "plain_seconds": pd,
+            "ratio_batched_over_plain": pd / bd,
+            "e2e": {"value": n_pri / bw, "seconds": bw, "plain_value": n_pri / pw, "plain_seconds": pw,
+                    "ratio_batched_over_plain": pw / bw,
+                    "what": "host primaries to host records, both arms (uploads, launches, record read-back)"},
+            "flights_per_s": c["flights"] / bd, "plain_flights_per_s": p_flights / pd,
+            "timing": "value / plain_value: transport kernels only (CUDA events), both arms",
+            "flights": c["flights"], "iterations": c["iterations"], "spilled": c["spilled"],
+            "records": int(sum(len(r) for r in recs_b)), "per_job_records_identical": bool(identical),
+            "se_total": int(sum(int((r["E"] < 50).sum()) for r in recs_b)),
+            "bse_total": int(sum(int((r["E"] >= 50).sum()) for r in recs_b)),
             "params": params, "launches_per_run": 1}
 
 
@@ -625,15 +657,26 @@ def run_case(args):
         sim = nb.Simulation(g, ms, capacity=args.capacity, seed=3, record_capacity=1 << 22, block_size=args.block,
                             step_mode=args.step_mode)
         runs = []
+        trace = []
         for r in range(args.repeat + 1):
             sim.reset()
             sim.push(w.primaries)
             t0 = time.perf_counter()
-            sim.run()
+            if r == 0 and args.trace_graphs:
+                # the first run graph by graph (24 iterations each), with the
+                # free flights each graph made: the launch index of an ncu
+                # capture maps to its graph, and so to its flights per launch
+                while True:
+                    left = sim.do_iteration(24)
+                    trace.append(sim.counters()["flights"])
+                    if left == 0:
+                        break
+            else:
+                sim.run()
             wall = time.perf_counter() - t0
             c = sim.counters()
             sim.flush_detected()
-            if r > 0:
+            if r > 0 or args.repeat == 0:
                 runs.append((sim.kernel_ms(), wall, c["flights"], c["iterations"]))
         sim.close()
     n = len(w.primaries)
@@ -641,7 +684,8 @@ def run_case(args):
     print(json.dumps({"case": "%s %dx%dx%d at %g eV" % (args.case, args.pixels, args.pixels, args.per_pixel, energy),
                       "primaries": n, "capacity": args.capacity, "step_mode": args.step_mode, "kernel_ms": kms,
                       "primaries_per_s": n / (kms / 1e3), "events_per_primary": runs[-1][2] / n,
-                      "iterations": runs[-1][3], "wall_s": float(np.mean([r[1] for r in runs]))}))
+                      "iterations": runs[-1][3], "wall_s": float(np.mean([r[1] for r in runs])),
+                      "flights_per_graph": list(np.diff([0] + trace).tolist()) if trace else None}))
 
 
 # ---------------------------------------------------------------------------- GPU
@@ -667,8 +711,10 @@ def main():
     ap.add_argument("--repeat", type=int, default=1, help="--case: timed runs after one warm-up run")
     ap.add_argument("--batch-scale", type=float, default=0.02, help="--case batch: fraction of every job's primaries")
     ap.add_argument("--block", type=int, default=0, help="--case: threads per block of the kernel (0: default)")
+    ap.add_argument("--trace-graphs", action="store_true",
+                    help="--case: run the first run graph by graph and report the flights of each graph")
     ap.add_argument("--step-mode", type=int, default=0, choices=[0, 1],
-                    help="wavefront iterations: 0 split (an item interacts or flies), 1 fused")
+                    help="wavefront iterations: 0 fused, 1 split (an item interacts or flies)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

@@ -235,8 +235,8 @@ typedef struct nbl_params {
 	uint32_t deposit_capacity;   /* deposit records buffered on the device; 0: no records */
 	nbl_deposit_grid deposit_grid; /* voxel grid of the losses; n = 0: none */
 	nbl_image_filter image_filter; /* detector acceptance of the per-pixel images */
-	int32_t step_mode;           /* 0: split wavefront (an iteration's item either interacts or flies);
-	                                1: fused (interaction and the next flight in one item); same results */
+	int32_t step_mode;           /* 0: fused wavefront (an item's interaction and its next flight in one
+	                                iteration); 1: split (an item either interacts or flies); same results */
 } nbl_params;
 void nbl_params_defaults(nbl_params* p);
 
@@ -378,6 +378,8 @@ typedef struct nbl_batch_params {
 	int32_t use_graph;         /* capture the launch in a CUDA graph; 0: plain launch */
 	void* stream;              /* NULL: a library-owned stream */
 	nbl_physics_opts physics;  /* one selection for every job */
+	uint32_t record_capacity;  /* detected records kept on the device for the whole batch, each with
+	                              its job (nbl_batch_records); 0: per-job yields only */
 } nbl_batch_params;
 void nbl_batch_params_defaults(nbl_batch_params* p);
 
@@ -392,6 +394,10 @@ nbl_status nbl_batch_set_jobs(nbl_batch* b, const nbl_batch_job* jobs, int32_t n
 nbl_status nbl_batch_run(nbl_batch* b);
 /* Detected electrons per job: se (E < 50 eV) and bse (E >= 50 eV), n_jobs each. */
 nbl_status nbl_batch_job_yields(nbl_batch* b, uint64_t* se, uint64_t* bse);
+/* The last run's detected records (the 36-byte records of gpu_main.cu:216-223,
+ * every job's, in detection order) and the job of each: n = how many; with
+ * cap = 0 only n is returned.  Needs record_capacity > 0. */
+nbl_status nbl_batch_records(nbl_batch* b, nbl_record* out, uint8_t* job, int64_t cap, int64_t* n);
 nbl_status nbl_batch_counters(nbl_batch* b, nbl_counters* out);
 /* Device time of the last run (CUDA events around the launch), ms. */
 nbl_status nbl_batch_kernel_ms(nbl_batch* b, double* ms);

@@ -92,7 +92,7 @@ class BatchParams(C.Structure):
     _fields_ = [("device", C.c_int32), ("capacity", C.c_uint32), ("refill_threshold", C.c_float),
                 ("block_size", C.c_uint32), ("queue_factor", C.c_uint32), ("energy_threshold", C.c_float),
                 ("max_events", C.c_uint32), ("max_iterations", C.c_uint32), ("use_graph", C.c_int32),
-                ("stream", C.c_void_p), ("physics", PhysicsOpts)]
+                ("stream", C.c_void_p), ("physics", PhysicsOpts), ("record_capacity", C.c_uint32)]
 
 
 COUNTER_NAMES = ("flights", "boundary", "elastic", "inelastic", "spawned", "detected", "terminated",
@@ -156,6 +156,7 @@ _DECLS = [
     ("nbl_batch_set_jobs", C.c_int, [C.c_void_p, C.POINTER(BatchJob), C.c_int32, C.c_void_p, C.c_int64]),
     ("nbl_batch_run", C.c_int, [C.c_void_p]),
     ("nbl_batch_job_yields", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("nbl_batch_records", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     ("nbl_batch_counters", C.c_int, [C.c_void_p, C.POINTER(Counters)]),
     ("nbl_batch_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("nbl_batch_destroy", None, [C.c_void_p]),

@@ -264,6 +264,7 @@ class Simulation:
             p.deposit_grid.n[:] = [int(v) for v in n]
             self.deposit_grid_shape = (int(n[2]), int(n[1]), int(n[0]))
         p.stream = stream
+        p.record_capacity = record_capacity
         self.params = p
         self.tally = tuple(tally)
         self.hist_bins = hist_bins
@@ -428,7 +429,7 @@ class Batch:
 
     def __init__(self, geometries, materials, capacity=1 << 20, refill_threshold=1.0, block_size=256,
                  queue_factor=4, device=0, use_graph=True, energy_threshold=0.0, max_events=0, stream=None,
-                 physics=None):
+                 physics=None, record_capacity=0):
         p = _capi.BatchParams()
         lib().nbl_batch_params_defaults(C.byref(p))
         p.physics = physics_options(physics)
@@ -441,6 +442,7 @@ class Batch:
         p.energy_threshold = energy_threshold
         p.max_events = max_events
         p.stream = stream
+        p.record_capacity = record_capacity
         self.params = p
         self.geometries = list(geometries)
         self.materials = list(materials)
@@ -453,8 +455,11 @@ class Batch:
         self._h = h
         self.n_jobs = 0
 
-    def set_jobs(self, jobs):
-        """``jobs``: list of (geometry index, seed, PRI_DTYPE primaries)."""
+    def set_jobs(self, jobs, primaries=None):
+        """``jobs``: list of (geometry index, seed, PRI_DTYPE primaries).
+        ``primaries``: optionally, the jobs' primaries already laid end to
+        end in one PRI_DTYPE array (then only the lengths of the jobs'
+        arrays are used)."""
         arr = (_capi.BatchJob * len(jobs))()
         first = 0
         for i, (gi, seed, pri) in enumerate(jobs):
@@ -463,7 +468,12 @@ class Batch:
             arr[i].first = first
             arr[i].count = len(pri)
             first += len(pri)
-        allp = np.ascontiguousarray(np.concatenate([np.asarray(p, PRI_DTYPE) for _, _, p in jobs]), PRI_DTYPE)
+        if primaries is None:
+            allp = np.ascontiguousarray(np.concatenate([np.asarray(p, PRI_DTYPE) for _, _, p in jobs]), PRI_DTYPE)
+        else:
+            allp = np.ascontiguousarray(primaries, PRI_DTYPE)
+            if len(allp) != first:
+                raise ValueError("primaries hold %d records, the jobs %d" % (len(allp), first))
         check(lib().nbl_batch_set_jobs(self._h, arr, len(jobs), allp.ctypes.data, len(allp)))
         self.n_jobs = len(jobs)
         self.n_primaries = len(allp)
@@ -476,6 +486,25 @@ class Batch:
         bse = (C.c_uint64 * self.n_jobs)()
         check(lib().nbl_batch_job_yields(self._h, se, bse))
         return np.array(se[:], np.int64), np.array(bse[:], np.int64)
+
+    def records(self):
+        """The last run's detected records (PRI_DTYPE) and the job of each
+        (uint8), in detection order; needs ``record_capacity``."""
+        n = C.c_int64()
+        check(lib().nbl_batch_records(self._h, None, None, 0, C.byref(n)))
+        rec = np.empty(n.value, PRI_DTYPE)
+        job = np.empty(n.value, np.uint8)
+        if n.value:
+            check(lib().nbl_batch_records(self._h, rec.ctypes.data, job.ctypes.data, n.value, C.byref(n)))
+        return rec, job
+
+    def job_records(self):
+        """The last run's detected records split by job: a list of n_jobs
+        PRI_DTYPE arrays (each in detection order)."""
+        rec, job = self.records()
+        order = np.argsort(job, kind="stable")
+        bounds = np.searchsorted(job[order], np.arange(self.n_jobs + 1))
+        return [rec[order[bounds[i]:bounds[i + 1]]] for i in range(self.n_jobs)]
 
     def counters(self):
         c = _capi.Counters()

@@ -773,8 +773,8 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		sp.max_events = params->max_events ? params->max_events : (1u << 22);
 		require(sp.max_events < (1u << 24), "max_events must be < 2^24");
 		sp.adjoint = adj ? 1 : 0;
-		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (split) or 1 (fused)");
-		sp.split = params->step_mode == 0 ? 1 : 0;
+		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (fused) or 1 (split)");
+		sp.split = params->step_mode;
 		s->grid = params->grid_size ? (int)params->grid_size : step_grid_size(s->device, s->block, sp);
 		s->ensure_primary_capacity(1024);
 		sp.n_primaries = 0;

@@ -2,6 +2,7 @@
 #include "internal.hpp"
 #include "device.hpp"
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 
@@ -18,6 +19,7 @@ struct nbl_batch {
 	DevBuf queues[2][N_QUEUES][4];
 	DevBuf spill[4];
 	DevBuf ctrl, counters, primaries, jobs, job_se, job_bse, words;
+	DevBuf detected, det_job, n_detected;     // detected records of the last run and their jobs
 	StepParams sp{};
 	BatchParams bp{};
 	int n_jobs = 0;
@@ -42,6 +44,8 @@ struct nbl_batch {
 		CU(cudaMemsetAsync(ctrl.p, 0, ctrl.bytes, stream));
 		CU(cudaMemsetAsync(counters.p, 0, counters.bytes, stream));
 		CU(cudaMemsetAsync(words.p, 0, words.bytes, stream));
+		if (n_detected.p)
+			CU(cudaMemsetAsync(n_detected.p, 0, n_detected.bytes, stream));
 		if (n_jobs) {
 			CU(cudaMemsetAsync(job_se.p, 0, job_se.bytes, stream));
 			CU(cudaMemsetAsync(job_bse.p, 0, job_bse.bytes, stream));
@@ -90,6 +94,9 @@ struct nbl_batch {
 			throw Error(NBL_ERR_CUDA, "batched launch: grid barrier timed out");
 		if (w[2] & 2u)
 			throw Error(NBL_ERR_BUDGET_EXCEEDED, "batched launch reached its iteration bound");
+		if (cnt[CNT_RECORD_OVERFLOW])
+			throw Error(NBL_ERR_POOL_OVERFLOW, std::to_string(cnt[CNT_RECORD_OVERFLOW]) +
+				" detected records did not fit; raise record_capacity");
 		if (cnt[CNT_QUEUE_OVERFLOW])
 			throw Error(NBL_ERR_POOL_OVERFLOW, std::to_string(cnt[CNT_QUEUE_OVERFLOW]) +
 				" electrons did not fit the overflow ring; raise capacity or queue_factor");
@@ -193,9 +200,22 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 		sp.ctrl = b->ctrl.as<uint32_t>();
 		b->counters.alloc(N_COUNTERS * sizeof(unsigned long long));
 		sp.counters = b->counters.as<unsigned long long>();
+		// detected records of every job in one buffer, each with its job
+		// beside it (the batch runs in one launch: the buffer holds the
+		// whole batch's records)
 		sp.detected = nullptr;
 		sp.n_detected = nullptr;
 		sp.det_cap = 0;
+		sp.det_job = nullptr;
+		if (params->record_capacity) {
+			b->detected.alloc((size_t)params->record_capacity * sizeof(Record36));
+			b->det_job.alloc((size_t)params->record_capacity);
+			b->n_detected.alloc(sizeof(uint32_t));
+			sp.detected = b->detected.as<Record36>();
+			sp.det_job = b->det_job.as<uint8_t>();
+			sp.n_detected = b->n_detected.as<uint32_t>();
+			sp.det_cap = params->record_capacity;
+		}
 		sp.tal = Tallies{};
 		sp.max_events = params->max_events ? params->max_events : (1u << 22);
 		require(sp.max_events < (1u << 24), "max_events must be < 2^24");
@@ -238,13 +258,16 @@ nbl_status nbl_batch_set_jobs(nbl_batch* b, const nbl_batch_job* jobs, int32_t n
 		}
 		require(prev_end == n_primaries, "job ranges must cover the primary array");
 		set_device(b->device);
-		b->jobs.alloc(dj.size() * sizeof(DevJob));
+		// device buffers are reused while large enough (a batch object is
+		// typically given job lists of similar size run after run)
+		auto fit = [](DevBuf& buf, size_t n) { if (buf.bytes < n) buf.alloc(n); };
+		fit(b->jobs, dj.size() * sizeof(DevJob));
 		CU(cudaMemcpy(b->jobs.p, dj.data(), dj.size() * sizeof(DevJob), cudaMemcpyHostToDevice));
-		b->primaries.alloc(std::max<int64_t>(n_primaries, 1) * sizeof(Record36));
+		fit(b->primaries, std::max<int64_t>(n_primaries, 1) * sizeof(Record36));
 		if (n_primaries)
 			CU(cudaMemcpy(b->primaries.p, primaries, n_primaries * sizeof(Record36), cudaMemcpyHostToDevice));
-		b->job_se.alloc(n_jobs * sizeof(unsigned long long));
-		b->job_bse.alloc(n_jobs * sizeof(unsigned long long));
+		fit(b->job_se, n_jobs * sizeof(unsigned long long));
+		fit(b->job_bse, n_jobs * sizeof(unsigned long long));
 		b->n_jobs = n_jobs;
 		b->sp.primaries = b->primaries.as<Record36>();
 		b->sp.n_primaries = (uint32_t)n_primaries;
@@ -276,6 +299,27 @@ nbl_status nbl_batch_job_yields(nbl_batch* b, uint64_t* se, uint64_t* bse)
 	});
 }
 
+nbl_status nbl_batch_records(nbl_batch* b, nbl_record* out, uint8_t* job, int64_t cap, int64_t* n)
+{
+	return guard([&] {
+		require(b && n, "null argument");
+		require(cap >= 0 && (cap == 0 || (out && job)), "bad output buffers");
+		require(b->n_detected.p != nullptr, "the batch keeps no records (record_capacity = 0)");
+		set_device(b->device);
+		uint32_t nd = 0;
+		CU(cudaMemcpy(&nd, b->n_detected.p, sizeof(nd), cudaMemcpyDeviceToHost));
+		const int64_t have = std::min<int64_t>(nd, b->sp.det_cap);
+		*n = have;
+		if (cap == 0)
+			return;
+		require(cap >= have, "output buffer holds " + std::to_string(cap) + " records, the run detected " +
+			std::to_string(have));
+		CU(cudaMemcpyAsync(out, b->detected.p, (size_t)have * sizeof(nbl_record), cudaMemcpyDeviceToHost, b->stream));
+		CU(cudaMemcpyAsync(job, b->det_job.p, (size_t)have, cudaMemcpyDeviceToHost, b->stream));
+		CU(cudaStreamSynchronize(b->stream));
+	});
+}
+
 nbl_status nbl_batch_counters(nbl_batch* b, nbl_counters* out)
 {
 	return guard([&] {
@@ -292,6 +336,11 @@ nbl_status nbl_batch_counters(nbl_batch* b, nbl_counters* out)
 		out->event_budget = c[CNT_EVENT_BUDGET]; out->spilled = c[CNT_SPILLED];
 		out->iterations = b->last_iterations;
 		out->primaries_total = b->sp.n_primaries;
+		if (b->n_detected.p) {
+			uint32_t nd = 0;
+			CU(cudaMemcpy(&nd, b->n_detected.p, sizeof(nd), cudaMemcpyDeviceToHost));
+			out->records_pending = std::min(nd, b->sp.det_cap);
+		}
 	});
 }
 

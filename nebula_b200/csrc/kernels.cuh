@@ -71,6 +71,7 @@ struct StepParams {
 	Record36* detected;
 	uint32_t* n_detected;
 	uint32_t det_cap;
+	uint8_t* det_job;         // batched runs: job of each detected record (null: none)
 	Tallies tal;
 	unsigned long long* counters;
 	uint32_t max_events;      // per-electron event budget

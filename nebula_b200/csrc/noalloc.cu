@@ -268,8 +268,8 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 
 		const int block = params->block_size ? (int)params->block_size : 256;
 		require(block % 32 == 0 && block >= 32 && block <= 256, "block_size must be a multiple of 32 in 32..256");
-		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (split) or 1 (fused)");
-		sp.split = params->step_mode == 0 ? 1 : 0;
+		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (fused) or 1 (split)");
+		sp.split = params->step_mode;
 		const int grid = params->grid_size ? (int)params->grid_size : step_grid_size(params->device, block, sp);
 		const uint32_t check_every = 24;
 		const uint64_t bound = 2ull * sp.max_events + (uint64_t)n_primaries + 64;

@@ -62,6 +62,25 @@ __device__ __forceinline__ uint32_t warp_reserve(uint32_t* counter, bool pred)
 	return base + (uint32_t)__popc(mask & lanemask_lt());
 }
 
+// Reserve one slot per lane in the queue `q` it names (0..3, -1: none) from
+// the four consecutive counters at `counters`; all 32 lanes must call.  The
+// atomics of the different queues are issued together (lane t issues queue
+// t's), so a warp that appends to several queues waits for one round trip
+// instead of one per queue.  Returns the lane's slot (undefined for q = -1).
+__device__ __forceinline__ uint32_t warp_reserve4(uint32_t* counters, int q)
+{
+	const unsigned m0 = __ballot_sync(0xffffffffu, q == 0), m1 = __ballot_sync(0xffffffffu, q == 1);
+	const unsigned m2 = __ballot_sync(0xffffffffu, q == 2), m3 = __ballot_sync(0xffffffffu, q == 3);
+	const uint32_t lane = threadIdx.x & 31u;
+	const unsigned issue = lane == 0u ? m0 : lane == 1u ? m1 : lane == 2u ? m2 : m3;
+	uint32_t base = 0;
+	if (lane < 4u && issue)
+		base = atomicAdd(counters + lane, (uint32_t)__popc(issue));
+	base = __shfl_sync(0xffffffffu, base, q > 0 ? q : 0);
+	const unsigned mq = q == 0 ? m0 : q == 1 ? m1 : q == 2 ? m2 : m3;
+	return base + (uint32_t)__popc(mq & lanemask_lt());
+}
+
 /* --------------------------------------------------------------- ray query */
 __global__ void k_ray_query(const DevGeometry g, const float* __restrict__ pos, const float* __restrict__ dir,
 	const float* __restrict__ dist, const int32_t* __restrict__ ignore_tri, const int32_t* __restrict__ ignore_mat,
@@ -433,8 +452,27 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 	if (lane == 0u) base = atomicAdd(work, 32u);
 	base = __shfl_sync(0xFFFFFFFFu, base, 0);
 
-	for (; base < total; ) {
-		const uint32_t item = base + lane;
+	// SPLIT: 32-item chunks of interactions (boundary, elastic, inelastic) and
+	// of flights (new, ring, primaries) alternate in the work order, so each
+	// SM keeps a mix of arithmetic-heavy and load-latency-bound warps
+	const uint32_t c_ev = (e2 + 31u) / 32u, c_fl = (total - e2 + 31u) / 32u;
+	const uint32_t c_mix = min(c_ev, c_fl);
+	const uint32_t limit = SPLIT ? (c_ev + c_fl) * 32u : total;
+	for (; base < limit; ) {
+		uint32_t item = base + lane;
+		if (SPLIT) {
+			const uint32_t j = base / 32u;
+			uint32_t at, end;
+			if (j < 2u * c_mix) {
+				at = (j & 1u) ? e2 + (j >> 1) * 32u : (j >> 1) * 32u;
+				end = (j & 1u) ? total : e2;
+			} else {
+				const uint32_t k = c_mix + (j - 2u * c_mix);
+				at = c_ev > c_fl ? k * 32u : e2 + k * 32u;
+				end = c_ev > c_fl ? e2 : total;
+			}
+			item = at + lane < end ? at + lane : total;
+		}
 		int kind = -1;
 		uint32_t qi = 0;
 		if (item < total) {
@@ -598,6 +636,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 					rec.dx = p.dir.x; rec.dy = p.dir.y; rec.dz = p.dir.z; rec.E = p.E;
 					rec.px = pr->px; rec.py = pr->py;
 					P.detected[rslot] = rec;
+					if (BATCH && P.det_job)
+						P.det_job[rslot] = (uint8_t)job;
 				} else {
 					lc.add(CNT_RECORD_OVERFLOW);
 				}
@@ -661,19 +701,20 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		}
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
 			lc.add(CNT_TERMINATED);
+		{
+			const uint32_t slot = warp_reserve4(cw, qtype);
+			if (qtype >= 0 && slot >= P.qcap)
+				lc.add(CNT_QUEUE_OVERFLOW);
+			// compile-time queue indices (a run-time index into the kernel
+			// parameters would copy them to local memory)
 #pragma unroll
-		for (int t = 0; t < (SPLIT ? 4 : 3); ++t) {
-			const bool mine = qtype == t;
-			const uint32_t slot = warp_reserve(cw + t, mine);
-			if (mine) {
-				if (slot < P.qcap) {
+			for (int t = 0; t < (SPLIT ? 4 : 3); ++t) {
+				if (qtype == t && slot < P.qcap) {
 					store_electron(qout[t], slot, p, mat, last_tri, tag, event, lineage);
 					if (ADJ) {
 						qout[t].s[slot] = make_float4(sc[0], sc[1], sc[2], sc[3]);
 						qout[t].s2[slot] = make_float2(sc[4], sc[5]);
 					}
-				} else {
-					lc.add(CNT_QUEUE_OVERFLOW);
 				}
 			}
 		}

@@ -91,3 +91,48 @@ def test_batch_rejects_bad_job_ranges(small_batch):
     with pytest.raises(nb.NblError):
         b.set_jobs(bad)
     b.close()
+
+
+def _plain_records(geoms, mats, jobs):
+    out = []
+    for gi, seed, pri in jobs:
+        sim = nb.Simulation(geoms[gi], mats[: (1 if gi == 0 else 2)], capacity=1 << 14, seed=seed)
+        sim.push(pri)
+        sim.run()
+        out.append(sim.flush_detected())
+        sim.close()
+    return out
+
+
+def _sorted(rec):
+    return np.sort(rec.view(np.dtype((np.void, 36))).ravel()).tobytes()
+
+
+def test_batch_records_equal_plain_runs(small_batch):
+    """Every job's detected 36-byte records from the batched launch equal, as
+    a set, the records of the job run alone in the plain wavefront."""
+    geoms, mats, jobs = small_batch
+    ref = _plain_records(geoms, mats, jobs)
+    b = nb.Batch(geoms, mats, capacity=1 << 14, block_size=256, record_capacity=1 << 20)
+    b.set_jobs(jobs)
+    for _ in range(2):
+        b.run()
+        per_job = b.job_records()
+        assert len(per_job) == len(jobs)
+        for k, (got, want) in enumerate(zip(per_job, ref)):
+            assert len(got) == len(want) > 0, k
+            assert _sorted(got) == _sorted(want), k
+        se, bse = b.job_yields()
+        assert np.array_equal(se, [int((r["E"] < 50).sum()) for r in ref])
+        assert b.counters()["records_pending"] == sum(len(r) for r in ref)
+    b.close()
+
+
+def test_batch_record_overflow_is_an_error(small_batch):
+    geoms, mats, jobs = small_batch
+    b = nb.Batch(geoms, mats, capacity=1 << 14, block_size=256, record_capacity=16)
+    b.set_jobs(jobs)
+    with pytest.raises(nb.NblError) as e:
+        b.run()
+    assert e.value.status == 6 and "record_capacity" in str(e.value)
+    b.close()

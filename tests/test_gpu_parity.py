@@ -250,16 +250,22 @@ def test_transport_deterministic_and_capacity_independent(inputs):
     pri = primaries.point_beam(3000)
     outs = []
     spilled = []
-    for cap, blk in ((1 << 16, 256), (1 << 12, 128), (64, 64)):
-        sim = nb.Simulation(g, [m], capacity=cap, seed=42, block_size=blk)
+    counters = []
+    # (pool capacity, threads per block, step mode: 0 fused, 1 split)
+    for cap, blk, mode in ((1 << 16, 256, 0), (1 << 12, 128, 0), (64, 64, 0), (1 << 16, 256, 1), (64, 64, 1)):
+        sim = nb.Simulation(g, [m], capacity=cap, seed=42, block_size=blk, step_mode=mode)
         sim.push(pri)
         sim.run()
         r = sim.flush_detected()
-        spilled.append(sim.counters()["spilled"])
-        outs.append(np.sort(r.view(np.dtype((np.void, 36))).ravel()))
-    assert outs[0].tobytes() == outs[1].tobytes() == outs[2].tobytes()
-    # the smallest pool must have parked secondaries in the overflow ring
-    assert spilled[2] > 0
+        c = sim.counters()
+        spilled.append(c["spilled"])
+        counters.append({k: c[k] for k in ("flights", "boundary", "elastic", "inelastic", "spawned", "detected",
+                                           "terminated", "primaries_started")})
+        outs.append(np.sort(r.view(np.dtype((np.void, 36))).ravel()).tobytes())
+    assert all(o == outs[0] for o in outs[1:])
+    assert all(c == counters[0] for c in counters[1:]), counters
+    # the smallest pools must have parked secondaries in the overflow ring
+    assert spilled[2] > 0 and spilled[4] > 0
 
 
 def test_small_capacity_forces_many_refills(inputs):
