@@ -53,6 +53,9 @@ typedef enum nbl_status {
 /* Message of the last failing call on this thread (never NULL). */
 const char* nbl_last_error_string(void);
 int nbl_abi_version(void);
+/* CUDA devices this process can use (0 without a driver or device); the
+ * reference's worker-per-GPU loop counts them the same way (gpu_main.cu:284-295). */
+nbl_status nbl_device_count(int32_t* n);
 
 /* Special material ids (core/material_manager.h:77-86). */
 #define NBL_MAT_NOP (-128)

@@ -109,6 +109,7 @@ class Counters(C.Structure):
 _DECLS = [
     ("nbl_last_error_string", C.c_char_p, []),
     ("nbl_abi_version", C.c_int, []),
+    ("nbl_device_count", C.c_int, [C.POINTER(C.c_int32)]),
     ("nbl_free", None, [C.c_void_p]),
     ("nbl_load_tri_file", C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Triangle)), i64p]),
     ("nbl_load_pri_file", C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Record)), i64p]),

@@ -20,15 +20,25 @@
 // energy before it, energy lost; pixel: cpu_energydep.cpp:197-204) and the
 // 36-byte detected records.
 //
-// It uses only the C ABI of include/nebula_b200.h.  Differences from the
-// reference drivers: no prescan (--prescan-size and --batch-factor are
-// accepted and ignored: the library keeps its pool full by itself), one
-// device per process (run one process per GPU on disjoint primaries), and
+// Like gpu_main.cu:284-295 it runs one worker thread per GPU (--devices:
+// all visible devices by default, or a list), each with its own simulation
+// handle; the workers pull contiguous ranges of the primary array from one
+// shared cursor (the reference's work_pool, gpu_main.cu:213) and each range
+// runs with its first primary's index as the primary offset, so every
+// primary draws the random numbers it draws in a one-GPU run and the records
+// are those of that run (in another order).  Records of all workers go out
+// through one writer thread (the reference's mutexed output stream).
+//
+// It uses only the C ABI of include/nebula_b200.h.  Other differences from
+// the reference drivers: no prescan (--prescan-size and --batch-factor are
+// accepted and ignored: the library keeps its pool full by itself), and
 // every primary is simulated (gpu_main.cu:228-229 can end a run one input
 // batch early when a frame starts with nothing in flight).
 #include "nebula_b200.h"
 
 #include <algorithm>
+#include <atomic>
+#include <deque>
 #include <chrono>
 #include <condition_variable>
 #include <mutex>
@@ -126,7 +136,9 @@ struct Timer {
 	}
 };
 
-// Writes record buffers to a stream on its own thread, one at a time.
+// Writes record buffers to a stream on its own thread, in the order they
+// are handed over (from any number of worker threads).  A buffer must not
+// change until its `done` flag is set (wait()).
 template<class T>
 class RecordWriter {
 public:
@@ -140,29 +152,37 @@ public:
 		cv_.notify_all();
 		thread_.join();
 	}
-	// hand over a buffer; it must not change until wait_idle() returns
-	void submit(const std::vector<T>* b)
+	void submit(const std::vector<T>* b, bool* done)
 	{
-		std::unique_lock<std::mutex> l(m_);
-		cv_.wait(l, [this] { return job_ == nullptr; });
+		std::lock_guard<std::mutex> l(m_);
 		rethrow();
-		job_ = b;
+		*done = false;
+		jobs_.push_back({ b, done });
 		cv_.notify_all();
 	}
-	void wait_idle()
+	// wait until the buffer whose flag this is has been written
+	void wait(const bool* done)
 	{
 		std::unique_lock<std::mutex> l(m_);
-		cv_.wait(l, [this] { return job_ == nullptr; });
+		cv_.wait(l, [&] { return *done || !error_.empty(); });
 		rethrow();
 	}
 	void finish()
 	{
-		wait_idle();
+		{
+			std::unique_lock<std::mutex> l(m_);
+			cv_.wait(l, [this] { return jobs_.empty() || !error_.empty(); });
+			rethrow();
+		}
 		if (std::fflush(f_) != 0)
 			throw std::runtime_error("writing records failed");
 	}
 
 private:
+	struct Job {
+		const std::vector<T>* b;
+		bool* done;
+	};
 	void rethrow()
 	{
 		if (!error_.empty())
@@ -172,16 +192,17 @@ private:
 	{
 		std::unique_lock<std::mutex> l(m_);
 		for (;;) {
-			cv_.wait(l, [this] { return job_ != nullptr || stop_; });
-			if (job_ == nullptr)
+			cv_.wait(l, [this] { return !jobs_.empty() || stop_; });
+			if (jobs_.empty())
 				return;
-			const std::vector<T>* b = job_;
+			const Job j = jobs_.front();
 			l.unlock();
-			const bool ok = b->empty() || std::fwrite(b->data(), sizeof(T), b->size(), f_) == b->size();
+			const bool ok = j.b->empty() || std::fwrite(j.b->data(), sizeof(T), j.b->size(), f_) == j.b->size();
 			l.lock();
 			if (!ok)
 				error_ = "writing records failed";
-			job_ = nullptr;
+			jobs_.pop_front();
+			*j.done = true;
 			cv_.notify_all();
 		}
 	}
@@ -189,7 +210,7 @@ private:
 	FILE* f_;
 	std::mutex m_;
 	std::condition_variable cv_;
-	const std::vector<T>* job_ = nullptr;
+	std::deque<Job> jobs_;
 	bool stop_ = false;
 	std::string error_;
 	std::thread thread_;
@@ -284,7 +305,11 @@ int run(int argc, char** argv)
 	cli.add("batch-factor", "0.9", "Accepted for compatibility; no input batches are sized");
 	cli.add("seed", "0x78c7e39b", "Random seed");
 	cli.add("sort-primaries", "0", "Sort primary electrons (Morton order of their positions) before simulation");
-	cli.add("device", "0", "CUDA device");
+	cli.add("device", "", "CUDA device to run on (one; overrides --devices)");
+	cli.add("devices", "all", "CUDA devices to run on, one worker thread each: all, or a comma-separated list");
+	cli.add("workers-per-device", "1", "Worker threads (simulation handles) per device");
+	cli.add("chunk", "0", "Primaries a worker takes from the shared queue at a time; 0: a quarter of an even share, "
+		"at least 65536");
 	cli.add("first-primary", "0", "Index of the file's first primary within a larger scan (resume, or one process "
 		"per GPU on disjoint files: the records equal one run over the whole scan)");
 	if (kEdep) {
@@ -403,7 +428,6 @@ int run(int argc, char** argv)
 
 	nbl_params p;
 	nbl_params_defaults(&p);
-	p.device = (int32_t)cli.u64("device");
 	p.capacity = (uint32_t)cli.u64("capacity");
 	p.energy_threshold = (float)cli.num("energy-threshold");
 	p.seed = cli.u64("seed");
@@ -419,8 +443,43 @@ int run(int argc, char** argv)
 	p.physics.interface_absorption = cli.flag("interface-absorption");
 	if (kEdep)
 		p.deposit_capacity = (uint32_t)cli.u64("deposit-buffer");
-	nbl_sim* sim = nullptr;
-	check(nbl_sim_create(geom, mats.data(), n_mat, &p, &sim), "creating the simulation");
+
+	// devices and workers (gpu_main.cu:284-295: one worker per visible GPU)
+	std::vector<int> devices;
+	if (!cli.get("device").empty()) {
+		devices.push_back((int)cli.u64("device"));
+	} else if (cli.get("devices") == "all") {
+		int32_t n_dev = 0;
+		check(nbl_device_count(&n_dev), "counting devices");
+		for (int d = 0; d < n_dev; ++d) devices.push_back(d);
+	} else {
+		const std::string& list = cli.get("devices");
+		size_t at = 0;
+		for (;;) {
+			const size_t comma = list.find(',', at);
+			const std::string item = list.substr(at, comma == std::string::npos ? std::string::npos : comma - at);
+			if (!item.empty()) devices.push_back(std::stoi(item));
+			if (comma == std::string::npos) break;
+			at = comma + 1;
+		}
+	}
+	if (devices.empty())
+		throw std::runtime_error("no CUDA device to run on");
+	const int per_device = std::max(1, (int)cli.u64("workers-per-device"));
+	std::vector<int> worker_device;
+	for (int d : devices)
+		for (int k = 0; k < per_device; ++k) worker_device.push_back(d);
+	const int n_workers = (int)worker_device.size();
+	int64_t chunk = (int64_t)cli.u64("chunk");
+	if (chunk <= 0)
+		chunk = std::max<int64_t>(65536, (n_pri + 4 * n_workers - 1) / (4 * n_workers));
+	std::vector<nbl_sim*> sims(n_workers, nullptr);
+	for (int w = 0; w < n_workers; ++w) {
+		p.device = worker_device[w];
+		check(nbl_sim_create(geom, mats.data(), n_mat, &p, &sims[w]), "creating the simulation");
+	}
+	std::fprintf(stderr, "Running on %d device(s), %d worker(s), %lld primaries per range.\n", (int)devices.size(),
+		n_workers, (long long)chunk);
 
 	// output streams: stdout for the detected records (gpu_main.cu) or the
 	// two files of cpu_energydep.cpp:169-170 ("stdout" = standard output)
@@ -438,78 +497,119 @@ int run(int argc, char** argv)
 	}
 
 	// the run, records streamed out as it goes (gpu_main.cu:191-231): each
-	// step's records are written by writer threads while the GPU runs the
-	// next step
+	// worker's records of one step are written by the writer threads while
+	// that worker runs its next step
 	timer.start();
-	check(nbl_sim_set_primary_offset(sim, cli.u64("first-primary")), "primary offset");
-	check(nbl_sim_push_primaries(sim, pri, n_pri), "pushing primaries");
-	nbl_free(pri);
-	int64_t written = 0, deposited = 0;
+	const uint64_t first_primary = cli.u64("first-primary");
+	std::atomic<int64_t> cursor{ 0 }, started{ 0 }, written{ 0 }, deposited{ 0 };
+	std::atomic<bool> failed{ false };
+	std::mutex err_m;
+	std::string error;
 	{
 		RecordWriter<nbl_record> writer(detect_f);
 		RecordWriter<nbl_deposit_record> dep_writer(deposit_f ? deposit_f : stdout);
-		std::vector<nbl_record> buf[2];
-		std::vector<nbl_deposit_record> dbuf[2];
-		int cur = 0;
-		auto drain = [&](std::vector<nbl_record>& out) {
-			int64_t pending = 0;
-			check(nbl_sim_detected_count(sim, &pending), "record count");
-			out.resize((size_t)pending);
-			int64_t got = 0;
-			while (got < pending) {
-				int64_t n = 0;
-				check(nbl_sim_drain_detected(sim, out.data() + got, pending - got, &n), "draining records");
-				if (n == 0) break;
-				got += n;
+		std::mutex progress_m;
+		auto worker = [&](int w) {
+			nbl_sim* sim = sims[w];
+			std::vector<nbl_record> buf[2];
+			std::vector<nbl_deposit_record> dbuf[2];
+			bool done[2] = { true, true }, ddone[2] = { true, true };
+			try {
+				int cur = 0;
+				auto drain = [&](std::vector<nbl_record>& out) {
+					int64_t pending = 0;
+					check(nbl_sim_detected_count(sim, &pending), "record count");
+					out.resize((size_t)pending);
+					int64_t got = 0;
+					while (got < pending) {
+						int64_t n = 0;
+						check(nbl_sim_drain_detected(sim, out.data() + got, pending - got, &n), "draining records");
+						if (n == 0) break;
+						got += n;
+					}
+					out.resize((size_t)got);
+					written += got;
+				};
+				auto drain_deposits = [&](std::vector<nbl_deposit_record>& out) {
+					nbl_counters c;
+					check(nbl_sim_counters(sim, &c), "counters");
+					out.resize((size_t)c.deposits_pending);
+					int64_t got = 0;
+					while (got < (int64_t)out.size()) {
+						int64_t n = 0;
+						check(nbl_sim_drain_deposits(sim, out.data() + got, (int64_t)out.size() - got, &n),
+							"draining deposits");
+						if (n == 0) break;
+						got += n;
+					}
+					out.resize((size_t)got);
+					deposited += got;
+				};
+				// ranges of the shared primary array, in turn
+				for (;;) {
+					const int64_t a = cursor.fetch_add(chunk);
+					if (a >= n_pri || failed)
+						break;
+					const int64_t n = std::min<int64_t>(chunk, n_pri - a);
+					check(nbl_sim_reset(sim), "reset");
+					check(nbl_sim_set_primary_offset(sim, first_primary + (uint64_t)a), "primary offset");
+					check(nbl_sim_push_primaries(sim, pri + a, n), "pushing primaries");
+					int64_t running = 1, seen = 0;
+					while (running > 0 && !failed) {
+						check(nbl_sim_step(sim, 240, &running), "transport");
+						writer.wait(&done[cur]);        // this buffer's previous records are out
+						drain(buf[cur]);
+						writer.submit(&buf[cur], &done[cur]);
+						if (kEdep) {
+							dep_writer.wait(&ddone[cur]);
+							drain_deposits(dbuf[cur]);
+							dep_writer.submit(&dbuf[cur], &ddone[cur]);
+						}
+						cur ^= 1;
+						nbl_counters c;
+						check(nbl_sim_counters(sim, &c), "counters");
+						started += (int64_t)c.primaries_started - seen;
+						seen = (int64_t)c.primaries_started;
+						std::lock_guard<std::mutex> l(progress_m);
+						std::fprintf(stderr, " \rProgress %.2f%% | Running: %lld",
+							100.0 * (double)started / (double)std::max<int64_t>(n_pri, 1), (long long)running);
+					}
+				}
+			} catch (const std::exception& e) {
+				std::lock_guard<std::mutex> l(err_m);
+				if (error.empty())
+					error = "device " + std::to_string(worker_device[w]) + ": " + e.what();
+				failed = true;
 			}
-			out.resize((size_t)got);
-			written += got;
+			// the writers may still hold this worker's buffers
+			for (int k = 0; k < 2; ++k) {
+				try { writer.wait(&done[k]); } catch (const std::exception&) { failed = true; }
+				if (kEdep)
+					try { dep_writer.wait(&ddone[k]); } catch (const std::exception&) { failed = true; }
+			}
 		};
-		auto drain_deposits = [&](std::vector<nbl_deposit_record>& out) {
-			nbl_counters c;
-			check(nbl_sim_counters(sim, &c), "counters");
-			out.resize((size_t)c.deposits_pending);
-			int64_t got = 0;
-			while (got < (int64_t)out.size()) {
-				int64_t n = 0;
-				check(nbl_sim_drain_deposits(sim, out.data() + got, (int64_t)out.size() - got, &n), "draining deposits");
-				if (n == 0) break;
-				got += n;
-			}
-			out.resize((size_t)got);
-			deposited += got;
-		};
-		int64_t running = 1;
-		while (running > 0) {
-			check(nbl_sim_step(sim, 240, &running), "transport");
-			writer.wait_idle();             // the other buffers are free again
-			drain(buf[cur]);
-			writer.submit(&buf[cur]);
-			if (kEdep) {
-				dep_writer.wait_idle();
-				drain_deposits(dbuf[cur]);
-				dep_writer.submit(&dbuf[cur]);
-			}
-			cur ^= 1;
-			nbl_counters c;
-			check(nbl_sim_counters(sim, &c), "counters");
-			std::fprintf(stderr, " \rProgress %.2f%% | Running: %lld",
-				100.0 * (double)c.primaries_started / (double)std::max<int64_t>(n_pri, 1), (long long)running);
-		}
+		std::vector<std::thread> threads;
+		for (int w = 0; w < n_workers; ++w)
+			threads.emplace_back(worker, w);
+		for (std::thread& t : threads)
+			t.join();
+		if (failed)
+			throw std::runtime_error(error.empty() ? std::string("writing records failed") : error);
 		writer.finish();
 		if (kEdep)
 			dep_writer.finish();
 	}
+	nbl_free(pri);
 	if (detect_f != stdout) std::fclose(detect_f);
 	if (deposit_f && deposit_f != stdout) std::fclose(deposit_f);
 	timer.stop("Simulation");
-	std::fprintf(stderr, "\nSimulation successful!\n%lld detected electrons written.\n", (long long)written);
+	std::fprintf(stderr, "\nSimulation successful!\n%lld detected electrons written.\n", (long long)written.load());
 	if (kEdep)
-		std::fprintf(stderr, "%lld energy deposits written.\n", (long long)deposited);
+		std::fprintf(stderr, "%lld energy deposits written.\n", (long long)deposited.load());
 	std::fprintf(stderr, "\n");
 	timer.print(stderr);
 
-	nbl_sim_destroy(sim);
+	for (nbl_sim* sim : sims) nbl_sim_destroy(sim);
 	for (nbl_material* m : mats) nbl_material_destroy(m);
 	nbl_geometry_destroy(geom);
 	return 0;

@@ -319,6 +319,20 @@ struct nbl_sim {
 extern "C" {
 
 const char* nbl_last_error_string(void) { return g_last_error.c_str(); }
+
+nbl_status nbl_device_count(int32_t* n)
+{
+	return guard([&] {
+		require(n != nullptr, "null argument");
+		int c = 0;
+		const cudaError_t e = cudaGetDeviceCount(&c);
+		if (e != cudaSuccess) {
+			cudaGetLastError();
+			c = 0;
+		}
+		*n = c;
+	});
+}
 int nbl_abi_version(void) { return NBL_ABI_VERSION; }
 void nbl_free(void* p) { std::free(p); }
 

@@ -48,6 +48,13 @@ class ScanProblem:
         self.adjoint_sim = Simulation(geometry, materials, capacity=capacity, seed=seed, tally=tally, device=device,
                                       adjoint=True, adjoint_w_step=self.w_step, physics=physics)
 
+    def set_seed(self, seed):
+        """Run both simulations with another random-number key (a new,
+        independent sample of the same scan)."""
+        self.forward_sim.set_seed(seed)
+        self.adjoint_sim.set_seed(seed)
+        self._forward_theta = None
+
     def theta0(self):
         return torch.tensor(self.forward_sim.get_theta(), dtype=torch.float64)
 

@@ -168,3 +168,35 @@ def test_split_files_with_first_primary_equal_one_run(driver, slab_files, tmp_pa
     assert whole.returncode == ra.returncode == rb.returncode == 0
     key = lambda buf: np.sort(np.frombuffer(buf, dtype=np.dtype((np.void, 36)))).tobytes()
     assert key(ra.stdout + rb.stdout) == key(whole.stdout)
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_no_device_is_an_error(driver, slab_files):
+    tri, pri, mat, _ = slab_files
+    r = _run([driver, tri, pri, mat])
+    assert r.returncode == 1 and r.stdout == b"" and b"no CUDA device" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
+def test_workers_sharing_the_primaries_equal_one_run(driver, slab_files, tmp_path):
+    """The worker-per-device fan-out (gpu_main.cu:284-295), run here as two
+    workers on device 0 taking 7001-primary ranges from the shared cursor:
+    the records equal, as a set, one worker's run over the whole file; the
+    same for the energy-deposit executable's two outputs."""
+    tri, pri, mat, p = slab_files
+    one = _run([driver, "--seed", "13", "--device", "0", tri, pri, mat])
+    two = _run([driver, "--seed", "13", "--devices", "0", "--workers-per-device", "2", "--chunk", "7001",
+                tri, pri, mat])
+    assert one.returncode == two.returncode == 0, two.stderr[-2000:]
+    assert b"2 worker(s)" in two.stderr
+    key = lambda buf, n: np.sort(np.frombuffer(buf, dtype=np.dtype((np.void, n)))).tobytes()
+    assert len(one.stdout) == len(two.stdout) > 0
+    assert key(two.stdout, 36) == key(one.stdout, 36)
+    d1, d2 = str(tmp_path / "d1.bin"), str(tmp_path / "d2.bin")
+    e1 = _run([build.DRIVER_EDEP, "--seed", "3", "--detect-filename", d1, tri, pri, mat])
+    e2 = _run([build.DRIVER_EDEP, "--seed", "3", "--detect-filename", d2, "--devices", "0",
+               "--workers-per-device", "2", "--chunk", "9000", tri, pri, mat])
+    assert e1.returncode == e2.returncode == 0, e2.stderr[-2000:]
+    assert key(e2.stdout, 28) == key(e1.stdout, 28)
+    assert key(open(d2, "rb").read(), 36) == key(open(d1, "rb").read(), 36)

@@ -4,9 +4,10 @@ central finite differences taken with common random numbers (same seed, so
 the runs share every random number): score-function estimates for the
 mean-free-path scales, the shifted-replay difference for the work functions.
 
-Tolerance: 5 % of the finite difference plus 3 standard errors of the
-difference, the error being estimated from the per-pixel spread (a pixel is
-an independent block of primaries).
+Tolerance of the gradient check: 5 % of the finite difference, on scans
+chosen so that 3 standard errors of the difference (estimated from the
+per-pixel spread, a pixel being an independent block of primaries) are at
+most 5 % of it.
 """
 import numpy as np
 import pytest
@@ -86,25 +87,71 @@ def test_adjoint_with_a_non_default_physics_selection(problem, physics):
     p0.close()
 
 
-@pytest.mark.parametrize("k", [0, 1, 2, 3, 4, 5])
-def test_gradients_match_crn_fd(problem, k):
-    th0 = problem.theta0().numpy()
-    w = problem.per_pixel
+def _resolving_problem(tmp_path_factory, which):
+    """A scan on which the parameters of one material carry a gradient that
+    a common-random-number difference resolves well within 5 %:
+    ``si``: 8.4 x 10^6 primaries at 500 eV on the 1 um Si slab (32 x 32
+    pixel groups of one point beam: independent blocks of primaries);
+    ``pmma``: 6.1 x 10^6 primaries at 500 eV on the grating's line-top
+    pixels (x beyond +-8 nm of the trench centre, 32 of the 64 columns).
+    On the whole grating field the Si inelastic gradient is a near
+    cancellation of its trench and line-top parts (~0.003), which no scan
+    of test size resolves to 5 %."""
+    from nebula_b200.synth import workloads, geometry, materials, nmat
+    from nebula_b200.torch_adjoint import ScanProblem
+    d = tmp_path_factory.mktemp("adj_" + which)
+    if which == "si":
+        w = workloads.slab(n_primaries=8 << 20, energy=500.0)
+        w.primaries["px"] = np.arange(len(w.primaries)) % 32
+        w.primaries["py"] = np.arange(len(w.primaries)) // 32 % 32
+        tally, n_mat = (32, 32), 1
+    else:
+        nx = 64
+        cols = list(range(0, 16)) + list(range(48, 64))
+        w = workloads.grating(nx=nx, ny=nx, per_pixel=3000,
+                              pixels=np.array([(x, y) for y in range(nx) for x in cols]))
+        tally, n_mat = (nx, nx), 2
+    tri = str(d / "g.tri")
+    geometry.write_tri(tri, w.triangles)
+    ms = []
+    for sp in w.material_specs[:n_mat]:
+        p = str(d / (sp.name + ".nmat"))
+        nmat.write(p, materials.build_raw_material(sp))
+        ms.append(nb.Material.load(p))
+    g = nb.Geometry.from_tri_file(tri)
+    return ScanProblem(g, ms, w.primaries, tally, seed=17, capacity=1 << 21), g, ms
+
+
+@pytest.mark.parametrize("which,ks", [("si", (0, 1, 2)), ("pmma", (3, 4, 5))])
+def test_gradients_match_crn_fd(tmp_path_factory, which, ks):
+    """Adjoint gradient of the total SE yield against the central difference
+    with common random numbers (5 % of a mean-free-path scale, 0.05 eV of a
+    work function), each on a scan where the difference is resolved: the
+    test asserts that it is (3 standard errors of adjoint - difference at
+    most 5 % of the difference) and then that the two agree within 5 %,
+    with no statistical allowance on top -- a 6 % bias in the adjoint
+    cannot pass.  The runs are deterministic (counter-based random
+    numbers), so the outcome is too."""
+    prob, g, ms = _resolving_problem(tmp_path_factory, which)
+    th0 = prob.theta0().numpy()
+    w = prob.per_pixel
     N = w.sum()
-    J = problem.jacobian(th0)
-    adj_pix = J[..., k] * w                  # per-pixel contributions to N * dY/dtheta_k
-    adj = adj_pix.sum() / N
-    delta = 0.05 if k % 3 == 2 else 0.01 * th0[k]
-    tp, tm = th0.copy(), th0.copy()
-    tp[k] += delta
-    tm[k] -= delta
-    yp = problem.forward(tp) * w
-    ym = problem.forward(tm) * w
-    fd_pix = (yp - ym) / (2 * delta)
-    fd = fd_pix.sum() / N
-    diff = (adj_pix - fd_pix).ravel()
-    se = diff.std(ddof=1) * np.sqrt(diff.size) / N
-    assert abs(adj - fd) <= 0.05 * abs(fd) + 3 * se, (k, adj, fd, se)
+    J = prob.jacobian(th0)
+    for k in ks:
+        adj_pix = (J[..., k] * w)[w > 0]     # per-pixel contributions to N * dY/dtheta_k
+        adj = adj_pix.sum() / N
+        delta = 0.05 if k % 3 == 2 else 0.05 * th0[k]
+        tp, tm = th0.copy(), th0.copy()
+        tp[k] += delta
+        tm[k] -= delta
+        fd_pix = ((prob.forward(tp) - prob.forward(tm)) * w / (2 * delta))[w > 0]
+        fd = fd_pix.sum() / N
+        diff = adj_pix - fd_pix
+        se = diff.std(ddof=1) * np.sqrt(diff.size) / N
+        assert 3 * se <= 0.05 * abs(fd), ("not resolved", k, adj, fd, se)
+        assert abs(adj - fd) <= 0.05 * abs(fd), (k, adj, fd, se)
+    prob.close()
+    g.close()
 
 
 def test_torch_autograd_matches_jacobian(problem):

@@ -8,12 +8,10 @@ CUDA path through the C ABI, different random numbers:
 * SE and BSE yields within 3 sigma (sigma from the spread over 500 primary
   groups in both runs);
 * detected energy distributions: two-sample KS on all records of both runs,
-  p > 0.001 -- the three energies here come on top of the workloads the
-  p > 0.01 criterion is applied to elsewhere, so the threshold keeps the
-  chance of a spurious failure of this family near 0.3 %; using every record
-  keeps the test's power (a 200 eV check against 2 x 10^6 GPU and 4 x 10^5
-  oracle primaries gave a binned KS distance of 0.0017, p ~ 0.6, and the
-  reference's own GPU driver agreed with both);
+  p > 0.01 (the criterion of the other parity tests); every record is used,
+  which keeps the test's power (a 200 eV check against 2 x 10^6 GPU and
+  4 x 10^5 oracle primaries gave a binned KS distance of 0.0017, p ~ 0.6,
+  and the reference's own GPU driver agreed with both);
 * events per primary within 3 %.
 """
 import os
@@ -52,9 +50,9 @@ def _group_totals(rec):
     return se, bse
 
 
-@pytest.mark.parametrize("energy,n_gpu,n_oracle", [(200.0, 400_000, 100_000),
-                                                   (5000.0, 200_000, 40_000),
-                                                   (15000.0, 100_000, 20_000)])
+@pytest.mark.parametrize("energy,n_gpu,n_oracle", [(200.0, 800_000, 200_000),
+                                                   (5000.0, 400_000, 80_000),
+                                                   (15000.0, 200_000, 40_000)])
 def test_yields_and_spectra_across_energies(tmp_path, energy, n_gpu, n_oracle):
     tri, mats, pri = _inputs(tmp_path, energy, n_gpu)
     g = nb.Geometry.from_tri_file(tri)
@@ -81,6 +79,6 @@ def test_yields_and_spectra_across_energies(tmp_path, energy, n_gpu, n_oracle):
         assert abs(ya - yb) < 3 * np.hypot(sa, sb), "%s yield at %g eV: %.5f vs oracle %.5f (sigma %.5f)" % (
             name, energy, ya, yb, np.hypot(sa, sb))
     p = stats.ks_2samp(ours["E"], ref["E"]).pvalue
-    assert p > 0.001, "energy spectra at %g eV: KS p = %.3g" % (energy, p)
+    assert p > 0.01, "energy spectra at %g eV: KS p = %.3g" % (energy, p)
     epp, epp_ref = flights / n_gpu, events / n_oracle
     assert abs(epp - epp_ref) < 0.03 * epp_ref, "events per primary %.1f vs oracle %.1f" % (epp, epp_ref)
