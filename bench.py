@@ -50,11 +50,16 @@ sys.path.insert(0, ROOT)
 
 METRIC = "primaries/s on 1 B200, plain vs batched; adjoint:forward time at yield err ≤3σ"
 BYTES_PER_EVENT = 96   # 48-byte electron state read + written per event
-# DRAM bytes (read + write) per event of the transport kernel on this workload,
-# from an ncu capture of one whole scan at the default pool (2^23):
-# dram__bytes_read.sum + dram__bytes_write.sum over its 96 launches / its
-# 1.4125e9 flights
-DRAM_BYTES_PER_EVENT = 89.8
+# DRAM bytes (read + write) per event of the transport kernel, measured on a
+# bounded case of this workload: the same grating scan at a pool of 2^20
+# (4.8 GB on the device), one whole graph of 6 launches in the middle of the
+# scan (launches 240-245, two ncu captures of 3 launches, warm L2:
+# --cache-control none), dram__bytes_read.sum + dram__bytes_write.sum over
+# those launches / the free flights of that graph (--trace-graphs).  It
+# exceeds the 96 algorithmic bytes because a flight whose walk continues in
+# the next iteration reads and writes its state again, plus 32 bytes of walk
+# state each way.
+DRAM_BYTES_PER_EVENT = 146.7
 
 
 def measured_peaks():
@@ -582,7 +587,7 @@ def rough_lines(args, dev, workdir):
     words = device_raster_scan(512, 512, 200, 0.5, 300.0, 40.0, 1.0, 11, dev)
     n = words.shape[0]
     sim = nb.Simulation(g, ms, capacity=args.capacity, seed=31, record_capacity=1 << 24, tally=(512, 512), device=dev,
-                        step_mode=args.step_mode)
+                        walk_cells=args.walk_cells)
     pri_dev = words
     sim.reset()
     sim.push_device(pri_dev.data_ptr(), n)
@@ -669,8 +674,9 @@ def run_case(args):
             tri = os.path.join(d, "g.tri")
             geometry.write_tri(tri, w.triangles)
             g = nb.Geometry.from_tri_file(tri)
-        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=3, record_capacity=1 << 22, block_size=args.block,
-                            step_mode=args.step_mode)
+        sim = nb.Simulation(g, ms, capacity=args.capacity, seed=3, record_capacity=1 << 24, block_size=args.block,
+                            iterations_per_graph=args.graph_iters,
+                            walk_cells=args.walk_cells)
         runs = []
         trace = []
         for r in range(args.repeat + 1):
@@ -678,11 +684,12 @@ def run_case(args):
             sim.push(w.primaries)
             t0 = time.perf_counter()
             if r == 0 and args.trace_graphs:
-                # the first run graph by graph (24 iterations each), with the
-                # free flights each graph made: the launch index of an ncu
-                # capture maps to its graph, and so to its flights per launch
+                # the first run graph by graph (--graph-iters iterations
+                # each), with the free flights each graph made: the launch
+                # index of an ncu capture maps to its graph, and so to its
+                # flights per launch
                 while True:
-                    left = sim.do_iteration(24)
+                    left = sim.do_iteration(args.graph_iters)
                     trace.append(sim.counters()["flights"])
                     if left == 0:
                         break
@@ -697,7 +704,8 @@ def run_case(args):
     n = len(w.primaries)
     kms = float(np.mean([r[0] for r in runs]))
     print(json.dumps({"case": "%s %dx%dx%d at %g eV" % (args.case, args.pixels, args.pixels, args.per_pixel, energy),
-                      "primaries": n, "capacity": args.capacity, "step_mode": args.step_mode, "kernel_ms": kms,
+                      "primaries": n, "capacity": args.capacity,
+                      "walk_cells": args.walk_cells, "kernel_ms": kms,
                       "primaries_per_s": n / (kms / 1e3), "events_per_primary": runs[-1][2] / n,
                       "iterations": runs[-1][3], "wall_s": float(np.mean([r[1] for r in runs])),
                       "flights_per_graph": list(np.diff([0] + trace).tolist()) if trace else None}))
@@ -726,10 +734,13 @@ def main():
     ap.add_argument("--repeat", type=int, default=1, help="--case: timed runs after one warm-up run")
     ap.add_argument("--batch-scale", type=float, default=0.02, help="--case batch: fraction of every job's primaries")
     ap.add_argument("--block", type=int, default=0, help="--case: threads per block of the kernel (0: default)")
+    ap.add_argument("--graph-iters", type=int, default=24,
+                    help="--case: wavefront iterations per CUDA graph (a multiple of 6)")
     ap.add_argument("--trace-graphs", action="store_true",
                     help="--case: run the first run graph by graph and report the flights of each graph")
-    ap.add_argument("--step-mode", type=int, default=0, choices=[0, 1],
-                    help="wavefront iterations: 0 fused, 1 split (an item interacts or flies)")
+    ap.add_argument("--walk-cells", type=int, default=0,
+                    help="leaf cells a flight's walk takes per iteration before continuing in the next (0: the "
+                         "library default, 1)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -760,7 +771,8 @@ def main():
         from nebula_b200 import replicas
         sim = nb.Simulation(g, ms, capacity=args.capacity, seed=replicas.replica_seed(1000, rank), device=dev,
                             tally=w.n_pixels,
-                            stream=stream.cuda_stream, record_capacity=args.record_capacity, step_mode=args.step_mode)
+                            stream=stream.cuda_stream, record_capacity=args.record_capacity,
+                            walk_cells=args.walk_cells)
         pri_dev = torch.from_numpy(w.primaries.view(np.uint8)).to(f"cuda:{dev}")
         pri_host = torch.from_numpy(w.primaries.view(np.uint8).copy()).pin_memory()
         rec_host = torch.empty(args.record_capacity * 36, dtype=torch.uint8).pin_memory()
@@ -797,6 +809,7 @@ def main():
         ev1 = torch.cuda.Event(enable_timing=True)
         kernel_ms = 0.0
         flights = 0
+        resumes = 0
         iters = 0
         detected = 0
         try:
@@ -808,6 +821,7 @@ def main():
                 c = sim.counters()
                 kernel_ms += sim.kernel_ms()
                 flights += c["flights"]
+                resumes += c["walk_resumes"]
                 iters += c["iterations"]
                 detected += c["detected"]
             ev1.record(stream)
@@ -854,12 +868,13 @@ def main():
                        "capacity": args.capacity, "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (primaries 236 MB, queues > 1 GB)"},
             "events_per_primary": flights / (n_pri * args.steps),
+            "walk_resumes_per_event": resumes / max(flights, 1),
             "detected_per_primary": detected / (n_pri * args.steps),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": DRAM_BYTES_PER_EVENT * flights / max(iters, 1),
-                         "traffic_unit": "bytes per launch (ncu capture of this workload, %.1f B per event)"
-                                         % DRAM_BYTES_PER_EVENT,
+                         "traffic_unit": "bytes per launch: %.1f B per event (ncu, one graph of the same scan at a "
+                                         "2^20 pool) x this run's events per launch" % DRAM_BYTES_PER_EVENT,
                          "note": "%d B algorithmic per event x %d events / transport-kernel time %.1f ms; "
                                  "peak %s" % (BYTES_PER_EVENT, flights, kernel_ms, peak_kind)},
             "e2e": {"value": e2e_value, "unit": "primaries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

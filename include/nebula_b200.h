@@ -238,8 +238,9 @@ typedef struct nbl_params {
 	uint32_t deposit_capacity;   /* deposit records buffered on the device; 0: no records */
 	nbl_deposit_grid deposit_grid; /* voxel grid of the losses; n = 0: none */
 	nbl_image_filter image_filter; /* detector acceptance of the per-pixel images */
-	int32_t step_mode;           /* 0: fused wavefront (an item's interaction and its next flight in one
-	                                iteration); 1: split (an item either interacts or flies); same results */
+	uint32_t walk_cells;         /* leaf cells a flight's octree walk takes per iteration; a longer walk
+	                                continues in the next iteration from where it stopped (same cells,
+	                                same float values, same results); 0: 1 */
 } nbl_params;
 void nbl_params_defaults(nbl_params* p);
 
@@ -257,6 +258,7 @@ typedef struct nbl_counters {
 	uint64_t deposits;           /* scatter events that deposited energy */
 	uint64_t deposit_overflow;   /* deposit records lost for lack of buffer room */
 	uint64_t deposits_pending;   /* deposit records not yet drained */
+	uint64_t walk_resumes;       /* flights whose walk continued in a later iteration (walk_cells) */
 } nbl_counters;
 
 nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
@@ -381,6 +383,7 @@ typedef struct nbl_batch_params {
 	int32_t use_graph;         /* capture the launch in a CUDA graph; 0: plain launch */
 	void* stream;              /* NULL: a library-owned stream */
 	nbl_physics_opts physics;  /* one selection for every job */
+	uint32_t walk_cells;       /* leaf cells a flight's walk takes per iteration (as nbl_params); 0: 1 */
 	uint32_t record_capacity;  /* detected records kept on the device for the whole batch, each with
 	                              its job (nbl_batch_records); 0: per-job yields only */
 } nbl_batch_params;
@@ -433,7 +436,7 @@ void nbl_batch_destroy(nbl_batch* b);
  * clears what must start at zero, and calls that overlap on the GPU race. */
 #define NBL_NOALLOC_MAX_CAPACITY 2048
 #define NBL_NOALLOC_MAX_MATERIALS 4
-#define NBL_NOALLOC_SCRATCH_BYTES 14813184
+#define NBL_NOALLOC_SCRATCH_BYTES 17565696
 nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const* materials, int32_t n_materials,
 	const nbl_params* params, const nbl_record* d_primaries, int64_t n_primaries, nbl_record* d_records,
 	int64_t records_cap, int64_t* n_records, uint32_t* d_se_img, uint32_t* d_bse_img, uint32_t* d_hist,

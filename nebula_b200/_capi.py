@@ -80,7 +80,7 @@ class Params(C.Structure):
                 ("hist_emax", C.c_float), ("max_events", C.c_uint32), ("stream", C.c_void_p),
                 ("physics", PhysicsOpts), ("adjoint", C.c_int32), ("adjoint_w_step", C.c_float),
                 ("deposit_capacity", C.c_uint32), ("deposit_grid", DepositGrid),
-                ("image_filter", ImageFilter), ("step_mode", C.c_int32)]
+                ("image_filter", ImageFilter), ("walk_cells", C.c_uint32)]
 
 
 class BatchJob(C.Structure):
@@ -92,13 +92,14 @@ class BatchParams(C.Structure):
     _fields_ = [("device", C.c_int32), ("capacity", C.c_uint32), ("refill_threshold", C.c_float),
                 ("block_size", C.c_uint32), ("queue_factor", C.c_uint32), ("energy_threshold", C.c_float),
                 ("max_events", C.c_uint32), ("max_iterations", C.c_uint32), ("use_graph", C.c_int32),
-                ("stream", C.c_void_p), ("physics", PhysicsOpts), ("record_capacity", C.c_uint32)]
+                ("stream", C.c_void_p), ("physics", PhysicsOpts), ("walk_cells", C.c_uint32),
+                ("record_capacity", C.c_uint32)]
 
 
 COUNTER_NAMES = ("flights", "boundary", "elastic", "inelastic", "spawned", "detected", "terminated",
                  "primaries_started", "walk_overflow", "nan_state", "queue_overflow",
                  "record_overflow", "event_budget", "spilled", "iterations", "primaries_total",
-                 "records_pending", "deposits", "deposit_overflow", "deposits_pending")
+                 "records_pending", "deposits", "deposit_overflow", "deposits_pending", "walk_resumes")
 
 
 class Counters(C.Structure):

@@ -233,7 +233,7 @@ class Simulation:
     def __init__(self, geometry, materials, capacity=1 << 20, seed=0x78C7E39B, energy_threshold=0.0, device=0,
                  tally=(0, 0), hist_bins=200, hist_emax=1000.0, record_capacity=0, block_size=0, grid_size=0,
                  iterations_per_graph=0, max_events=0, adjoint=False, stream=None, physics=None,
-                 adjoint_w_step=0.0, deposit_capacity=0, deposit_grid=None, image_cos_range=None, step_mode=0):
+                 adjoint_w_step=0.0, deposit_capacity=0, deposit_grid=None, image_cos_range=None, walk_cells=0):
         p = _capi.Params()
         lib().nbl_params_defaults(C.byref(p))
         p.physics = physics_options(physics)
@@ -252,7 +252,7 @@ class Simulation:
         p.adjoint = int(bool(adjoint))
         p.adjoint_w_step = adjoint_w_step
         p.deposit_capacity = deposit_capacity
-        p.step_mode = step_mode
+        p.walk_cells = walk_cells
         if image_cos_range is not None:
             p.image_filter.enabled = 1
             p.image_filter.cos_min, p.image_filter.cos_max = (float(v) for v in image_cos_range)
@@ -265,6 +265,7 @@ class Simulation:
             self.deposit_grid_shape = (int(n[2]), int(n[1]), int(n[0]))
         p.stream = stream
         p.record_capacity = record_capacity
+        p.walk_cells = walk_cells
         self.params = p
         self.tally = tuple(tally)
         self.hist_bins = hist_bins
@@ -429,7 +430,7 @@ class Batch:
 
     def __init__(self, geometries, materials, capacity=1 << 20, refill_threshold=1.0, block_size=256,
                  queue_factor=4, device=0, use_graph=True, energy_threshold=0.0, max_events=0, stream=None,
-                 physics=None, record_capacity=0):
+                 physics=None, record_capacity=0, walk_cells=0):
         p = _capi.BatchParams()
         lib().nbl_batch_params_defaults(C.byref(p))
         p.physics = physics_options(physics)

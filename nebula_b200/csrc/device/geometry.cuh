@@ -84,21 +84,48 @@ __device__ __forceinline__ bool in_domain(const DevGeometry& g, float x, float y
 		&& (z > fs(g.cz, g.hz)) && (z < fa(g.cz, g.hz));
 }
 
+// Where a walk stands between leaf cells: the current point, the distance
+// left, the location code of the cell it is about to enter and the cells
+// walked so far.  A walk cut short after some cells resumes from this state
+// with exactly the float values it would have carried on with.
+struct WalkState {
+	float cx, cy, cz, to_go;
+	uint64_t location;
+	int steps;
+};
+
+__device__ __forceinline__ WalkState walk_start(float sx, float sy, float sz, float distance)
+{
+	WalkState w;
+	w.cx = sx; w.cy = sy; w.cz = sz; w.to_go = distance;
+	w.location = 1;
+	w.steps = 0;
+	return w;
+}
+
+// Status of a walk that stopped at its cell budget (propagate_cells).
+#define NBL_WALK_PENDING (-3)
+
 // Nearest triangle hit within `distance` along a (normalised) direction,
 // ignoring `ignore_tri` and triangles whose outgoing material equals
-// `ignore_mat`.  Returns the triangle index (or -1) and the distance (or
-// `distance` itself when nothing is hit).  A walk longer than `max_steps`
-// leaf cells stops early and reports -2 (the host counts these as errors;
-// the reference has no such bound).
-__device__ __forceinline__ int propagate(const DevGeometry& g, float sx, float sy, float sz,
+// `ignore_mat`, walking from state `w` (walk_start for a new walk).  Returns
+// the triangle index (or -1) and the distance (or `distance` itself when
+// nothing is hit).  A walk longer than `max_steps` leaf cells in all stops
+// early and reports -2 (the host counts these as errors; the reference has no
+// such bound).  With `max_cells` > 0, a walk that has not ended after
+// `max_cells` cells in this call returns NBL_WALK_PENDING with `w` holding
+// where it stands; calling again with that state continues the same cell
+// sequence with the same float values.
+__device__ __forceinline__ int propagate_cells(const DevGeometry& g, WalkState& w,
 	float dx, float dy, float dz, float distance, int ignore_tri, int ignore_mat, float& out_dist,
-	int max_steps = 1 << 20)
+	int max_cells = 0, int max_steps = 1 << 20)
 {
 	const int32_t* __restrict__ od = g.octree;
-	float cx = sx, cy = sy, cz = sz;
-	float to_go = distance;
-	uint64_t location = 1;
-	int steps = 0;
+	float cx = w.cx, cy = w.cy, cz = w.cz;
+	float to_go = w.to_go;
+	uint64_t location = w.location;
+	int steps = w.steps;
+	int cells = 0;
 	do {
 		// Cell centre update of the reference, c += (aw * h) * (bit - 0.5)
 		// with aw = 2^-level: both products are exact (power-of-two
@@ -192,9 +219,25 @@ __device__ __forceinline__ int propagate(const DevGeometry& g, float sx, float s
 			out_dist = distance;
 			return -2;
 		}
+		if (++cells == max_cells && location > 1) {
+			w.cx = cx; w.cy = cy; w.cz = cz; w.to_go = to_go;
+			w.location = location;
+			w.steps = steps;
+			out_dist = distance;
+			return NBL_WALK_PENDING;
+		}
 	} while (location > 1);
 	out_dist = distance;
 	return -1;
+}
+
+// The whole walk in one call (octree<gpu_flag>::propagate).
+__device__ __forceinline__ int propagate(const DevGeometry& g, float sx, float sy, float sz,
+	float dx, float dy, float dz, float distance, int ignore_tri, int ignore_mat, float& out_dist,
+	int max_steps = 1 << 20)
+{
+	WalkState w = walk_start(sx, sy, sz, distance);
+	return propagate_cells(g, w, dx, dy, dz, distance, ignore_tri, ignore_mat, out_dist, 0, max_steps);
 }
 
 }  // namespace nbl

@@ -97,10 +97,16 @@ __device__ __forceinline__ V3 make_normal_vec(V3 dir, float phi)
 	return vadd(vmul(unit_u, cp), vmul(unit_v, sp));
 }
 
+// Inverse mean free path scale * exp(table(log E)).
+__device__ __forceinline__ float imfp_at(const DevTable& imfp_tab, float scale, float E)
+{
+	return fm(scale, __expf(table1_get(imfp_tab, __logf(E))));
+}
+
 // One exponential free path: -tau * log(U), tau = 1 / (scale * exp(table(log E)))
 template<class R> __device__ __forceinline__ float sample_path(const DevTable& imfp_tab, float scale, float E, R& rng, float& mu)
 {
-	mu = fm(scale, __expf(table1_get(imfp_tab, __logf(E))));
+	mu = imfp_at(imfp_tab, scale, E);
 	const float tau = fdf(1.0f, mu);
 	return fm(-tau, __logf(rng.unit()));
 }

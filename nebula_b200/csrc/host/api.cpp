@@ -69,7 +69,7 @@ struct nbl_sim {
 	nbl_params params{};
 	DeviceGeometry geom;
 	DeviceMaterials mats;
-	DevBuf queues[2][N_QUEUES][6];
+	DevBuf queues[2][N_QUEUES][8];
 	DevBuf spill[6];
 	DevBuf ctrl, counters, detected, n_detected, se_img, bse_img, hist, grad_se, grad_bse, wsign_se, wsign_bse;
 	DevBuf deposits, n_deposits, dep_grid;
@@ -224,7 +224,7 @@ struct nbl_sim {
 					deposits_seen = ndep;
 				}
 			}
-			const uint64_t active = (uint64_t)c[0] + c[1] + c[2] + c[3] + spill_occupancy(c);
+			const uint64_t active = queued(c) + spill_occupancy(c);
 			const uint64_t left = n_pri - c[SLOT_CURSOR];
 			if (active == 0 && left == 0)
 				return 0;
@@ -240,7 +240,14 @@ struct nbl_sim {
 			last_progress = progress;
 		}
 		read_ctrl(c);
-		return (int64_t)((uint64_t)c[0] + c[1] + c[2] + c[3] + spill_occupancy(c) + (n_pri - c[SLOT_CURSOR]));
+		return (int64_t)(queued(c) + spill_occupancy(c) + (n_pri - c[SLOT_CURSOR]));
+	}
+
+	static uint64_t queued(const uint32_t* c)
+	{
+		uint64_t n = 0;
+		for (int q = 0; q < N_QUEUES; ++q) n += c[q];
+		return n;
 	}
 
 	static uint32_t spill_occupancy(const uint32_t* c)
@@ -248,12 +255,13 @@ struct nbl_sim {
 		return c[SLOT_SPILL_TAIL] + c[SLOT_SPILL_PUSHED] - c[SLOT_SPILL_HEAD];
 	}
 
+	// flights started plus walks continued: grows in every iteration that has work
 	uint64_t flights_done()
 	{
-		unsigned long long f = 0;
-		CU(cudaMemcpyAsync(&f, counters.as<unsigned long long>() + CNT_FLIGHTS, sizeof(f), cudaMemcpyDeviceToHost, stream));
+		unsigned long long c[N_COUNTERS];
+		CU(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
 		CU(cudaStreamSynchronize(stream));
-		return f;
+		return c[CNT_FLIGHTS] + c[CNT_RESUMED];
 	}
 
 	void check_errors()
@@ -680,6 +688,8 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		sp.refill_below = cap;
 		sp.phys = phys;
 		const bool adj = params->adjoint != 0;
+		require(params->walk_cells <= (1u << 20), "walk_cells must be at most 2^20");
+		sp.walk_cells = params->walk_cells ? params->walk_cells : 1u;
 		for (int b = 0; b < 2; ++b)
 			for (int q = 0; q < N_QUEUES; ++q) {
 				DevBuf* qb = s->queues[b][q];
@@ -694,6 +704,11 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 				Queue& Q = sp.q[b][q];
 				Q.a = qb[0].as<float4>(); Q.b = qb[1].as<float4>(); Q.c = qb[2].as<uint4>(); Q.d = qb[3].as<uint32_t>();
 				Q.s = qb[4].as<float4>(); Q.s2 = qb[5].as<float2>();
+				if (q == EV_WALK) {
+					qb[6].alloc((size_t)sp.qcap * sizeof(float4));
+					qb[7].alloc((size_t)sp.qcap * sizeof(uint4));
+				}
+				Q.w0 = qb[6].as<float4>(); Q.w1 = qb[7].as<uint4>();
 			}
 		{
 			// overflow ring: at least twice the population bound, >= 2^20
@@ -711,6 +726,7 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 			Queue& Q = sp.spill;
 			Q.a = qb[0].as<float4>(); Q.b = qb[1].as<float4>(); Q.c = qb[2].as<uint4>(); Q.d = qb[3].as<uint32_t>();
 			Q.s = qb[4].as<float4>(); Q.s2 = qb[5].as<float2>();
+			Q.w0 = nullptr; Q.w1 = nullptr;
 			sp.spill_mask = ring - 1;
 		}
 		s->ctrl.alloc(3 * SLOT_WORDS * sizeof(uint32_t));
@@ -787,8 +803,6 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		sp.max_events = params->max_events ? params->max_events : (1u << 22);
 		require(sp.max_events < (1u << 24), "max_events must be < 2^24");
 		sp.adjoint = adj ? 1 : 0;
-		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (fused) or 1 (split)");
-		sp.split = params->step_mode;
 		s->grid = params->grid_size ? (int)params->grid_size : step_grid_size(s->device, s->block, sp);
 		s->ensure_primary_capacity(1024);
 		sp.n_primaries = 0;
@@ -858,10 +872,13 @@ nbl_status nbl_sim_run(nbl_sim* s)
 	return guard([&] {
 		require(s != nullptr, "null simulation");
 		set_device(s->device);
-		// the budget bounds the iterations: an electron cannot outlive
-		// max_events flights (two iterations each when split), and the pool
-		// refills at least one primary per iteration while primaries are left
-		const uint64_t bound = 2ull * s->sp.max_events + s->n_pri + 16;
+		// a safety bound on the iterations (the stall check and the walk's
+		// step bound are what end a run that cannot progress): an electron
+		// cannot outlive max_events flights, a flight's walk continues over
+		// cells / walk_cells iterations (64 covers the walks met here many
+		// times over), and the pool refills at least one primary per
+		// iteration while primaries are left
+		const uint64_t bound = ((uint64_t)s->sp.max_events + 1) * 64 + s->n_pri + 16;
 		const uint64_t max_graphs = bound / s->graph_iters + 2;
 		const int64_t left = s->advance(max_graphs);
 		s->check_errors();
@@ -1016,6 +1033,7 @@ nbl_status nbl_sim_counters(nbl_sim* s, nbl_counters* out)
 			CU(cudaStreamSynchronize(s->stream));
 		}
 		out->deposits_pending = s->host_deposits.size() + std::min(nd, s->sp.dep_cap);
+		out->walk_resumes = c[CNT_RESUMED];
 	});
 }
 

@@ -16,7 +16,7 @@ struct nbl_batch {
 	std::vector<std::unique_ptr<DeviceGeometry>> geoms;
 	DevBuf geom_views;
 	DeviceMaterials mats;
-	DevBuf queues[2][N_QUEUES][4];
+	DevBuf queues[2][N_QUEUES][6];
 	DevBuf spill[4];
 	DevBuf ctrl, counters, primaries, jobs, job_se, job_bse, words;
 	DevBuf detected, det_job, n_detected;     // detected records of the last run and their jobs
@@ -175,6 +175,8 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 		sp.ramp = std::max<uint32_t>(cap / 16, 256);
 		sp.refill_below = std::max<uint32_t>(1u, (uint32_t)((double)thr * cap));
 		sp.phys = phys;
+		require(params->walk_cells <= (1u << 20), "walk_cells must be at most 2^20");
+		sp.walk_cells = params->walk_cells ? params->walk_cells : 1u;
 		for (int k = 0; k < 2; ++k)
 			for (int q = 0; q < N_QUEUES; ++q) {
 				DevBuf* qb = b->queues[k][q];
@@ -184,7 +186,12 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 				qb[3].alloc((size_t)sp.qcap * sizeof(uint32_t));
 				Queue& Q = sp.q[k][q];
 				Q.a = qb[0].as<float4>(); Q.b = qb[1].as<float4>(); Q.c = qb[2].as<uint4>(); Q.d = qb[3].as<uint32_t>();
-				Q.s = nullptr; Q.s2 = nullptr;
+				Q.s = nullptr; Q.s2 = nullptr; Q.w0 = nullptr; Q.w1 = nullptr;
+				if (q == EV_WALK) {
+					qb[4].alloc((size_t)sp.qcap * sizeof(float4));
+					qb[5].alloc((size_t)sp.qcap * sizeof(uint4));
+					Q.w0 = qb[4].as<float4>(); Q.w1 = qb[5].as<uint4>();
+				}
 			}
 		uint32_t ring = 1u << 20;
 		while (ring < 2 * sp.qcap) ring <<= 1;
@@ -194,7 +201,7 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 		b->spill[3].alloc((size_t)ring * sizeof(uint32_t));
 		sp.spill.a = b->spill[0].as<float4>(); sp.spill.b = b->spill[1].as<float4>();
 		sp.spill.c = b->spill[2].as<uint4>(); sp.spill.d = b->spill[3].as<uint32_t>();
-		sp.spill.s = nullptr; sp.spill.s2 = nullptr;
+		sp.spill.s = nullptr; sp.spill.s2 = nullptr; sp.spill.w0 = nullptr; sp.spill.w1 = nullptr;
 		sp.spill_mask = ring - 1;
 		b->ctrl.alloc(3 * SLOT_WORDS * sizeof(uint32_t));
 		sp.ctrl = b->ctrl.as<uint32_t>();

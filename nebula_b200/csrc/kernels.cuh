@@ -17,25 +17,28 @@ struct Queue {
 	uint32_t* d;    // lineage hi
 	float4* s;      // adjoint: scores d log p / d theta, parameters 0..3 (null if off)
 	float2* s2;     // adjoint: parameters 4..5
+	float4* w0;     // EV_WALK only: walk point x, y, z, distance left
+	uint4* w1;      //   location code lo, hi, flight length (float bits), type | hop << 2 | cells << 4
 };
 
 // Counters kept on the device (64-bit).
 enum : int {
 	CNT_FLIGHTS = 0, CNT_BOUNDARY, CNT_ELASTIC, CNT_INELASTIC, CNT_SPAWNED, CNT_DETECTED,
 	CNT_TERMINATED, CNT_PRIMARIES, CNT_WALK_OVERFLOW, CNT_NAN, CNT_QUEUE_OVERFLOW,
-	CNT_RECORD_OVERFLOW, CNT_EVENT_BUDGET, CNT_SPILLED, CNT_DEPOSITS, CNT_DEPOSIT_OVERFLOW, N_COUNTERS
+	CNT_RECORD_OVERFLOW, CNT_EVENT_BUDGET, CNT_SPILLED, CNT_DEPOSITS, CNT_DEPOSIT_OVERFLOW, CNT_RESUMED, N_COUNTERS
 };
 
 // Per-iteration control words, three rotating slots of 16 words:
-// [queue counts x4, primary cursor, secondary tickets, spill head, spill tail
-//  at iteration start, spill pushes this iteration, pad].
+// [queue counts x N_QUEUES, primary cursor, secondary tickets, spill head,
+//  spill tail at iteration start, spill pushes this iteration, work, pad].
 constexpr int SLOT_WORDS = 16;
-constexpr int SLOT_CURSOR = 4;
-constexpr int SLOT_TICKETS = 5;
-constexpr int SLOT_SPILL_HEAD = 6;
-constexpr int SLOT_SPILL_TAIL = 7;
-constexpr int SLOT_SPILL_PUSHED = 8;
-constexpr int SLOT_WORK = 9;          // items handed out so far in the iteration that reads the slot
+constexpr int SLOT_CURSOR = N_QUEUES;
+constexpr int SLOT_TICKETS = N_QUEUES + 1;
+constexpr int SLOT_SPILL_HEAD = N_QUEUES + 2;
+constexpr int SLOT_SPILL_TAIL = N_QUEUES + 3;
+constexpr int SLOT_SPILL_PUSHED = N_QUEUES + 4;
+constexpr int SLOT_WORK = N_QUEUES + 5;   // items handed out so far in the iteration that reads the slot
+static_assert(SLOT_WORK < SLOT_WORDS, "control slot too small");
 
 struct Tallies {
 	uint32_t* se_img;        // per pixel counts of detected E < 50 eV (null: off)
@@ -86,7 +89,7 @@ struct StepParams {
 	double* grid;             // eV per voxel [gn[2]][gn[1]][gn[0]]
 	float g_org[3], g_inv[3]; // grid origin, 1 / voxel size
 	int32_t gn[3];
-	int32_t split;            // 1: split iterations (an item interacts or flies), 0: fused
+	uint32_t walk_cells;      // leaf cells a flight's walk takes per iteration before it continues in the next
 };
 
 // Work-function sign of a primary for material m (0 or 1): +1 or -1 from a

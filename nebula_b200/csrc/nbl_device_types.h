@@ -16,8 +16,11 @@ enum : int32_t {
 struct PhiloxKey { uint32_t k0, k1; };
 
 // Event kinds.  The queue order is the order events are laid out in the
-// per-iteration index space of the transport kernel.
-enum : int32_t { EV_BOUNDARY = 0, EV_ELASTIC = 1, EV_INELASTIC = 2, EV_NEW = 3, N_QUEUES = 4 };
+// per-iteration index space of the transport kernel.  EV_NEW holds electrons
+// whose next action is a free flight (new secondaries; in split iterations
+// also electrons after their interaction); EV_WALK flights whose octree walk
+// stopped at the per-iteration cell budget and continues.
+enum : int32_t { EV_BOUNDARY = 0, EV_ELASTIC = 1, EV_INELASTIC = 2, EV_NEW = 3, EV_WALK = 4, N_QUEUES = 5 };
 
 // One triangle, 64 bytes, four 16-byte vectors so a warp fetches it with
 // 128-bit loads: (r0, material_in) (e1, material_out) (e2, 0) (normal, 0).

@@ -57,7 +57,11 @@ constexpr size_t OFF_MATS = align_up(OFF_NDET + sizeof(uint32_t));
 constexpr size_t OFF_GEOM = align_up(OFF_MATS + NBL_NOALLOC_MAX_MATERIALS * sizeof(DevMaterial));
 constexpr size_t OFF_TABLES = OFF_GEOM + NA_GEOM_BYTES;
 constexpr size_t OFF_QUEUES = OFF_TABLES + NA_TABLE_BYTES;
-constexpr size_t OFF_SPILL = OFF_QUEUES + 2 * N_QUEUES * QUEUE_BYTES(NA_QCAP);
+// the event, flight and walk-continuation queues; the last also carries the
+// walk state of a flight that continues (two more 16-byte words per entry)
+constexpr size_t WALK_BYTES(uint32_t n) { return 2 * align_up((size_t)n * 16); }
+constexpr size_t OFF_WALK = OFF_QUEUES + 2 * N_QUEUES * QUEUE_BYTES(NA_QCAP);
+constexpr size_t OFF_SPILL = OFF_WALK + 2 * WALK_BYTES(NA_QCAP);
 constexpr size_t SCRATCH_BYTES = OFF_SPILL + QUEUE_BYTES(NA_RING);
 static_assert(SCRATCH_BYTES == NBL_NOALLOC_SCRATCH_BYTES, "NBL_NOALLOC_SCRATCH_BYTES out of date");
 static_assert((NA_RING & (NA_RING - 1)) == 0, "ring size must be a power of two");
@@ -92,6 +96,8 @@ Queue carve_queue(unsigned char* base, uint32_t n)
 	q.d = reinterpret_cast<uint32_t*>(base + 3 * align_up((size_t)n * 16));
 	q.s = nullptr;
 	q.s2 = nullptr;
+	q.w0 = nullptr;
+	q.w1 = nullptr;
 	return q;
 }
 
@@ -119,6 +125,7 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		require(n_materials >= 1 && n_materials <= NBL_NOALLOC_MAX_MATERIALS,
 			"nbl_run_noalloc: at most " + std::to_string(NBL_NOALLOC_MAX_MATERIALS) + " materials");
 		require(params->adjoint == 0, "nbl_run_noalloc: the adjoint is not available without allocation");
+		require(params->walk_cells <= (1u << 20), "walk_cells must be at most 2^20");
 		const nbl_deposit_grid& dgp = params->deposit_grid;
 		require(params->deposit_capacity == 0 && dgp.n[0] == 0 && dgp.n[1] == 0 && dgp.n[2] == 0,
 			"nbl_run_noalloc: energy deposits are not available without allocation");
@@ -237,6 +244,11 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 		for (int b = 0; b < 2; ++b)
 			for (int q = 0; q < N_QUEUES; ++q, qb += QUEUE_BYTES(NA_QCAP))
 				sp.q[b][q] = carve_queue(qb, NA_QCAP);
+		for (int b = 0; b < 2; ++b) {
+			unsigned char* wb = base + OFF_WALK + b * WALK_BYTES(NA_QCAP);
+			sp.q[b][EV_WALK].w0 = reinterpret_cast<float4*>(wb);
+			sp.q[b][EV_WALK].w1 = reinterpret_cast<uint4*>(wb + align_up((size_t)NA_QCAP * 16));
+		}
 		sp.qcap = 8 * cap;
 		sp.capacity = cap;
 		sp.ramp = std::max<uint32_t>(cap / 16, 256);
@@ -268,11 +280,10 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 
 		const int block = params->block_size ? (int)params->block_size : 256;
 		require(block % 32 == 0 && block >= 32 && block <= 256, "block_size must be a multiple of 32 in 32..256");
-		require(params->step_mode == 0 || params->step_mode == 1, "step_mode must be 0 (fused) or 1 (split)");
-		sp.split = params->step_mode;
+		sp.walk_cells = params->walk_cells ? params->walk_cells : 1u;
 		const int grid = params->grid_size ? (int)params->grid_size : step_grid_size(params->device, block, sp);
 		const uint32_t check_every = 24;
-		const uint64_t bound = 2ull * sp.max_events + (uint64_t)n_primaries + 64;
+		const uint64_t bound = ((uint64_t)sp.max_events + 1) * 64 + (uint64_t)n_primaries + 64;
 		uint32_t ctrl[SLOT_WORDS];
 		unsigned long long flights = 0, last_flights = ~0ull;
 		int stalled = 0;
@@ -286,8 +297,9 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 			cuda_ok(cudaMemcpyAsync(&flights, sp.counters + CNT_FLIGHTS, sizeof(flights), cudaMemcpyDeviceToHost, s),
 				"read state");
 			cuda_ok(cudaStreamSynchronize(s), "transport");
-			const uint64_t active = (uint64_t)ctrl[0] + ctrl[1] + ctrl[2] + ctrl[3] +
-				(uint32_t)(ctrl[SLOT_SPILL_TAIL] + ctrl[SLOT_SPILL_PUSHED] - ctrl[SLOT_SPILL_HEAD]);
+			uint64_t active = (uint32_t)(ctrl[SLOT_SPILL_TAIL] + ctrl[SLOT_SPILL_PUSHED] - ctrl[SLOT_SPILL_HEAD]);
+			for (int q = 0; q < N_QUEUES; ++q)
+				active += ctrl[q];
 			done = active == 0 && ctrl[SLOT_CURSOR] == (uint32_t)n_primaries;
 			if (!done) {
 				stalled = flights == last_flights ? stalled + 1 : 0;

@@ -62,22 +62,23 @@ __device__ __forceinline__ uint32_t warp_reserve(uint32_t* counter, bool pred)
 	return base + (uint32_t)__popc(mask & lanemask_lt());
 }
 
-// Reserve one slot per lane in the queue `q` it names (0..3, -1: none) from
-// the four consecutive counters at `counters`; all 32 lanes must call.  The
+// Reserve one slot per lane in the queue `q` it names (0..4, -1: none) from
+// the five consecutive counters at `counters`; all 32 lanes must call.  The
 // atomics of the different queues are issued together (lane t issues queue
 // t's), so a warp that appends to several queues waits for one round trip
 // instead of one per queue.  Returns the lane's slot (undefined for q = -1).
-__device__ __forceinline__ uint32_t warp_reserve4(uint32_t* counters, int q)
+__device__ __forceinline__ uint32_t warp_reserve5(uint32_t* counters, int q)
 {
 	const unsigned m0 = __ballot_sync(0xffffffffu, q == 0), m1 = __ballot_sync(0xffffffffu, q == 1);
 	const unsigned m2 = __ballot_sync(0xffffffffu, q == 2), m3 = __ballot_sync(0xffffffffu, q == 3);
+	const unsigned m4 = __ballot_sync(0xffffffffu, q == 4);
 	const uint32_t lane = threadIdx.x & 31u;
-	const unsigned issue = lane == 0u ? m0 : lane == 1u ? m1 : lane == 2u ? m2 : m3;
+	const unsigned issue = lane == 0u ? m0 : lane == 1u ? m1 : lane == 2u ? m2 : lane == 3u ? m3 : m4;
 	uint32_t base = 0;
-	if (lane < 4u && issue)
+	if (lane < 5u && issue)
 		base = atomicAdd(counters + lane, (uint32_t)__popc(issue));
 	base = __shfl_sync(0xffffffffu, base, q > 0 ? q : 0);
-	const unsigned mq = q == 0 ? m0 : q == 1 ? m1 : q == 2 ? m2 : m3;
+	const unsigned mq = q == 0 ? m0 : q == 1 ? m1 : q == 2 ? m2 : q == 3 ? m3 : m4;
 	return base + (uint32_t)__popc(mq & lanemask_lt());
 }
 
@@ -212,44 +213,106 @@ struct RunView {
 	PhiloxKey key;
 };
 
+// What a flight whose walk stopped at the cell budget carries to the next
+// iteration (the EV_WALK queue's w0 / w1 words).
+struct FlightResume {
+	WalkState w;
+	float dist;      // the flight's length (sampled, or the domain extent in vacuum)
+	int type;        // what ends it if no triangle does: 0 nothing (vacuum), 1 inelastic, 2 elastic
+	int hop;
+};
+
+__device__ __forceinline__ void load_resume(const Queue& q, uint32_t i, FlightResume& fr)
+{
+	const float4 w0 = __ldcg(q.w0 + i);
+	const uint4 w1 = __ldcg(q.w1 + i);
+	fr.w.cx = w0.x; fr.w.cy = w0.y; fr.w.cz = w0.z; fr.w.to_go = w0.w;
+	fr.w.location = ((uint64_t)w1.y << 32) | w1.x;
+	fr.dist = __uint_as_float(w1.z);
+	fr.type = (int)(w1.w & 3u);
+	fr.hop = (int)((w1.w >> 2) & 3u);
+	fr.w.steps = (int)(w1.w >> 4);
+}
+
+__device__ __forceinline__ void store_resume(const Queue& q, uint32_t i, const FlightResume& fr)
+{
+	q.w0[i] = make_float4(fr.w.cx, fr.w.cy, fr.w.cz, fr.w.to_go);
+	q.w1[i] = make_uint4((uint32_t)fr.w.location, (uint32_t)(fr.w.location >> 32), __float_as_uint(fr.dist),
+		(uint32_t)fr.type | ((uint32_t)fr.hop << 2) | ((uint32_t)fr.w.steps << 4));
+}
+
 // Free flight(s) from the electron's current state: domain and energy cut,
 // free-path sampling, octree walk, move.  Flights in vacuum that hit nothing
 // end without an event and are repeated (the next one leaves the domain).
-// Returns the queue of the event the flight ends in, or -1 when the electron
-// is terminated.  Mirrors cpu_driver::init / kernels::init
+// Returns the queue of the event the flight ends in, -1 when the electron is
+// terminated, or EV_WALK when the walk reached the run's per-iteration cell
+// budget (`fr` then holds where it stands).  With `resume` non-null, the
+// flight stored at entry `resume_i` of that walk queue continues (its checks,
+// event count and random draws are behind it).
+// Mirrors cpu_driver::init / kernels::init
 // (drivers/cpu/cpu_driver.inl:74-130, drivers/gpu/gpu_driver.inl:403-480).
 template<bool ADJ>
 __device__ __forceinline__ int free_flight(const StepParams& P, const RunView& rv, Electron& p, int mat, int& last_tri,
-	uint32_t& event, uint32_t stream_tag, uint64_t lineage, float* sc, LocalCounters& lc, const float* dbar = nullptr)
+	uint32_t& event, uint32_t stream_tag, uint64_t lineage, float* sc, LocalCounters& lc, const float* dbar,
+	FlightResume& fr, const Queue* resume, uint32_t resume_i)
 {
 	const DevGeometry& G = *rv.geom;
-	for (int hop = 0; hop < 4; ++hop) {
-		lc.add(CNT_FLIGHTS);
-		if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) { lc.add(CNT_NAN); return -1; }
-		if (!in_domain(G, p.pos.x, p.pos.y, p.pos.z))
-			return -1;
-		if (event >= P.max_events) { lc.add(CNT_EVENT_BUDGET); return -1; }
-		++event;
+	if (resume) {
+		load_resume(*resume, resume_i, fr);
+		lc.add(CNT_RESUMED);
+	}
+	for (int hop = resume ? fr.hop : 0; hop < 4; ++hop) {
 		int type = 0;
-		float dist = G.max_extent;
+		float dist;
 		float mu_el = 0.0f, mu_in = 0.0f;
 		const DevMaterial* m = nullptr;
-		if (mat >= 0) {
-			m = P.mats + mat;
-			const float barrier = (ADJ && dbar && mat < 2) ? fa(m->barrier, dbar[mat]) : m->barrier;
-			if (p.E < fa(barrier, P.energy_threshold))
+		WalkState w;
+		if (resume) {
+			resume = nullptr;
+			type = fr.type;
+			dist = fr.dist;
+			w = fr.w;
+			if (mat >= 0) {
+				m = P.mats + mat;
+				if (ADJ) {
+					// the inverse mean free paths the flight was sampled with
+					mu_el = imfp_at(m->el_imfp, m->el_scale, p.E);
+					mu_in = imfp_at(m->in_imfp, m->in_scale, p.E);
+				}
+			}
+		} else {
+			lc.add(CNT_FLIGHTS);
+			if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) { lc.add(CNT_NAN); return -1; }
+			if (!in_domain(G, p.pos.x, p.pos.y, p.pos.z))
 				return -1;
-			PhiloxStream r;
-			r.init(rv.key, event, 0u, stream_tag, lineage);
-			const float pe = sample_path(m->el_imfp, m->el_scale, p.E, r, mu_el);
-			const float pi = sample_path(m->in_imfp, m->in_scale, p.E, r, mu_in);
-			dist = __int_as_float(0x7f800000);
-			if (pe < dist) { dist = pe; type = 2; }
-			if (pi < dist) { dist = pi; type = 1; }
+			if (event >= P.max_events) { lc.add(CNT_EVENT_BUDGET); return -1; }
+			++event;
+			dist = G.max_extent;
+			if (mat >= 0) {
+				m = P.mats + mat;
+				const float barrier = (ADJ && dbar && mat < 2) ? fa(m->barrier, dbar[mat]) : m->barrier;
+				if (p.E < fa(barrier, P.energy_threshold))
+					return -1;
+				PhiloxStream r;
+				r.init(rv.key, event, 0u, stream_tag, lineage);
+				const float pe = sample_path(m->el_imfp, m->el_scale, p.E, r, mu_el);
+				const float pi = sample_path(m->in_imfp, m->in_scale, p.E, r, mu_in);
+				dist = __int_as_float(0x7f800000);
+				if (pe < dist) { dist = pe; type = 2; }
+				if (pi < dist) { dist = pi; type = 1; }
+			}
+			w = walk_start(p.pos.x, p.pos.y, p.pos.z, dist);
 		}
 		const V3 d = vnormalised(p.dir);
 		float idist;
-		const int hit = propagate(G, p.pos.x, p.pos.y, p.pos.z, d.x, d.y, d.z, dist, last_tri, mat, idist);
+		const int hit = propagate_cells(G, w, d.x, d.y, d.z, dist, last_tri, mat, idist, (int)P.walk_cells);
+		if (hit == NBL_WALK_PENDING) {
+			fr.w = w;
+			fr.dist = dist;
+			fr.type = type;
+			fr.hop = hop;
+			return EV_WALK;
+		}
 		if (hit == -2) { lc.add(CNT_WALK_OVERFLOW); return -1; }
 		if (ADJ && mat >= 0 && mat < 2) {
 			// score of the flight: density mu_k exp(-(mu_in+mu_el) d) of the
@@ -271,34 +334,6 @@ __device__ __forceinline__ int free_flight(const StepParams& P, const RunView& r
 		if (type == 2) return EV_ELASTIC;
 	}
 	return -1;
-}
-
-// Whether the free flight of an electron that survived its interaction gets
-// past the checks at the top of free_flight's first hop (state only, no
-// random draw): a split iteration makes the decision at the interaction, so
-// that only electrons that will walk are queued for a flight.  Counts what
-// free_flight would count for an electron that stops there.
-template<bool ADJ>
-__device__ __forceinline__ bool flight_starts(const StepParams& P, const RunView& rv, const Electron& p, int mat,
-	uint32_t event, LocalCounters& lc, const float* dbar)
-{
-	bool go = true;
-	if (!(p.E == p.E) || !(p.pos.x == p.pos.x)) {
-		lc.add(CNT_NAN);
-		go = false;
-	} else if (!in_domain(*rv.geom, p.pos.x, p.pos.y, p.pos.z)) {
-		go = false;
-	} else if (event >= P.max_events) {
-		lc.add(CNT_EVENT_BUDGET);
-		go = false;
-	} else if (mat >= 0) {
-		const DevMaterial* m = P.mats + mat;
-		const float barrier = (ADJ && dbar && mat < 2) ? fa(m->barrier, dbar[mat]) : m->barrier;
-		go = !(p.E < fa(barrier, P.energy_threshold));
-	}
-	if (!go)
-		lc.add(CNT_FLIGHTS);
-	return go;
 }
 
 __device__ __forceinline__ void store_electron(const Queue& q, uint32_t slot, const Electron& p, int mat, int last_tri,
@@ -379,17 +414,7 @@ __device__ __forceinline__ void deposit(const StepParams& P, bool scat, const El
 		lc.add(CNT_DEPOSITS);
 }
 
-// SPLIT: an item either interacts or flies, never both.  Items of the
-// boundary / elastic / inelastic queues perform their interaction and, if the
-// electron goes on, queue it in the flight queue (EV_NEW) of the next
-// iteration; items of the flight queue, the drained ring and the new
-// primaries perform a free flight and queue the electron for the event it
-// ends in.  Every lane of a flight-segment warp then walks the octree (the
-// electrons that end at their interaction -- detected, absorbed, below the
-// escape cut -- no longer idle their lanes through the walks of the others),
-// at the price of an extra queue pass per event.  Each electron's sequence
-// of events and random numbers is the same either way.
-template<bool ADJ, bool BATCH, bool DEP = false, uint32_t PHC = 0u, bool SPLIT = false>
+template<bool ADJ, bool BATCH, bool DEP = false, uint32_t PHC = 0u>
 __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc,
 	float* s_lane = nullptr)
 {
@@ -404,8 +429,9 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 	// keeps them there; the clamp makes an out-of-range read impossible)
 	const uint32_t n0 = min(ld_ctrl(cr + 0), P.qcap), n1 = min(ld_ctrl(cr + 1), P.qcap);
 	const uint32_t n2 = min(ld_ctrl(cr + 2), P.qcap), n3 = min(ld_ctrl(cr + 3), P.qcap);
+	const uint32_t n4 = min(ld_ctrl(cr + 4), P.qcap);
 	const uint32_t cursor = ld_ctrl(cr + SLOT_CURSOR);
-	const uint32_t e1 = n0 + n1, e2 = e1 + n2, active = e2 + n3;
+	const uint32_t e1 = n0 + n1, e2 = e1 + n2, e2n = e2 + n3, active = e2n + n4;
 	// spill ring: secondaries that found no room earlier, drained (oldest
 	// first) ahead of new primaries while the population has room
 	const uint32_t sp_head = ld_ctrl(cr + SLOT_SPILL_HEAD);
@@ -452,36 +478,21 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 	if (lane == 0u) base = atomicAdd(work, 32u);
 	base = __shfl_sync(0xFFFFFFFFu, base, 0);
 
-	// SPLIT: 32-item chunks of interactions (boundary, elastic, inelastic) and
-	// of flights (new, ring, primaries) alternate in the work order, so each
-	// SM keeps a mix of arithmetic-heavy and load-latency-bound warps
-	const uint32_t c_ev = (e2 + 31u) / 32u, c_fl = (total - e2 + 31u) / 32u;
-	const uint32_t c_mix = min(c_ev, c_fl);
-	const uint32_t limit = SPLIT ? (c_ev + c_fl) * 32u : total;
-	for (; base < limit; ) {
-		uint32_t item = base + lane;
-		if (SPLIT) {
-			const uint32_t j = base / 32u;
-			uint32_t at, end;
-			if (j < 2u * c_mix) {
-				at = (j & 1u) ? e2 + (j >> 1) * 32u : (j >> 1) * 32u;
-				end = (j & 1u) ? total : e2;
-			} else {
-				const uint32_t k = c_mix + (j - 2u * c_mix);
-				at = c_ev > c_fl ? k * 32u : e2 + k * 32u;
-				end = c_ev > c_fl ? e2 : total;
-			}
-			item = at + lane < end ? at + lane : total;
-		}
+	for (; base < total; ) {
+		const uint32_t item = base + lane;
+		// item kinds: the queues EV_BOUNDARY .. EV_WALK, then K_RING (a
+		// secondary drained from the spill ring) and K_PRIMARY (a new primary)
+		constexpr int K_RING = N_QUEUES, K_PRIMARY = N_QUEUES + 1;
 		int kind = -1;
 		uint32_t qi = 0;
 		if (item < total) {
 			if (item < n0) { kind = EV_BOUNDARY; qi = item; }
 			else if (item < e1) { kind = EV_ELASTIC; qi = item - n0; }
 			else if (item < e2) { kind = EV_INELASTIC; qi = item - e1; }
-			else if (item < active) { kind = EV_NEW; qi = item - e2; }
-			else if (item < e3) { kind = 5; qi = (sp_head + (item - active)) & P.spill_mask; }
-			else { kind = 4; qi = cursor + (item - e3); }
+			else if (item < e2n) { kind = EV_NEW; qi = item - e2; }
+			else if (item < active) { kind = EV_WALK; qi = item - e2n; }
+			else if (item < e3) { kind = K_RING; qi = (sp_head + (item - active)) & P.spill_mask; }
+			else { kind = K_PRIMARY; qi = cursor + (item - e3); }
 		}
 
 		Electron p;
@@ -491,8 +502,9 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		float sc[6];
 #pragma unroll
 		for (int k = 0; k < 6; ++k) sc[k] = 0.0f;
-		if (kind == 5 || (kind >= 0 && kind < 4)) {
-			const Queue& q = kind == 5 ? P.spill : qin[kind];
+		FlightResume fr;
+		if (kind == K_RING || (kind >= 0 && kind < N_QUEUES)) {
+			const Queue& q = kind == K_RING ? P.spill : qin[kind];
 			const float4 a = __ldcg(q.a + qi), b = __ldcg(q.b + qi);
 			const uint4 c = __ldcg(q.c + qi);
 			p.pos = v3(a.x, a.y, a.z); p.E = a.w;
@@ -504,7 +516,7 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 				const float2 s2 = __ldcg(q.s2 + qi);
 				sc[0] = s.x; sc[1] = s.y; sc[2] = s.z; sc[3] = s.w; sc[4] = s2.x; sc[5] = s2.y;
 			}
-		} else if (kind == 4) {
+		} else if (kind == K_PRIMARY) {
 			const Record36* r = P.primaries + qi;
 			p.pos = v3(r->x, r->y, r->z);
 			p.dir = v3(r->dx, r->dy, r->dz);
@@ -689,32 +701,29 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			}
 		}
 
-		// next free flight (SPLIT: the flight queue, for electrons that
-		// interacted in this item)
+		// next free flight (or the rest of a walk cut short last iteration)
 		int qtype = -1;
-		if (status == ST_RUNNING) {
-			if (SPLIT && kind < EV_NEW)
-				qtype = flight_starts<ADJ>(P, rv, p, mat, event, lc, wshift ? dbar : nullptr) ? EV_NEW : -1;
-			else
-				qtype = free_flight<ADJ>(P, rv, p, mat, last_tri, event, stream_tag, lineage, sc, lc,
-					wshift ? dbar : nullptr);
-		}
+		if (status == ST_RUNNING)
+			qtype = free_flight<ADJ>(P, rv, p, mat, last_tri, event, stream_tag, lineage, sc, lc,
+				wshift ? dbar : nullptr, fr, kind == EV_WALK ? &qin[EV_WALK] : nullptr, qi);
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
 			lc.add(CNT_TERMINATED);
 		{
-			const uint32_t slot = warp_reserve4(cw, qtype);
+			const uint32_t slot = warp_reserve5(cw, qtype);
 			if (qtype >= 0 && slot >= P.qcap)
 				lc.add(CNT_QUEUE_OVERFLOW);
 			// compile-time queue indices (a run-time index into the kernel
 			// parameters would copy them to local memory)
 #pragma unroll
-			for (int t = 0; t < (SPLIT ? 4 : 3); ++t) {
+			for (int t = 0; t < N_QUEUES; ++t) {
 				if (qtype == t && slot < P.qcap) {
 					store_electron(qout[t], slot, p, mat, last_tri, tag, event, lineage);
 					if (ADJ) {
 						qout[t].s[slot] = make_float4(sc[0], sc[1], sc[2], sc[3]);
 						qout[t].s2[slot] = make_float2(sc[4], sc[5]);
 					}
+					if (t == EV_WALK)
+						store_resume(qout[t], slot, fr);
 				}
 			}
 		}
@@ -738,7 +747,7 @@ __device__ __forceinline__ void flush_counters(const StepParams& P, uint32_t* s_
 // DEP: energy deposits on (a separate instantiation, so the plain step keeps
 // none of their code).  PHC: nonzero = the physics selection fixed at
 // compile time (PH_DEFAULT only).
-template<bool ADJ, bool DEP, uint32_t PHC = 0u, bool SPLIT = false>
+template<bool ADJ, bool DEP, uint32_t PHC = 0u>
 __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
@@ -748,7 +757,7 @@ __global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepPar
 	__syncthreads();
 	LocalCounters lc{ s_counters };
 	const BatchParams none{};
-	step_iteration<ADJ, false, DEP, PHC, SPLIT>(P, none, it, lc, s_lane);
+	step_iteration<ADJ, false, DEP, PHC>(P, none, it, lc, s_lane);
 	flush_counters(P, s_counters);
 }
 
@@ -814,25 +823,19 @@ __global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const Batc
 
 // The step kernel instantiation a run's parameters select: adjoint or not,
 // deposits or not, the default physics selection fixed at compile time or the
-// run-time word, split or fused iterations.
-template<bool SPLIT>
-static const void* step_kernel_for(const StepParams& p)
+// run-time word.
+static const void* step_kernel(const StepParams& p)
 {
 	const bool dep = p.dep || p.grid;
 	const bool fixed = p.phys == PH_DEFAULT;
 	if (p.adjoint) {
-		if (dep) return (const void*)k_step<true, true, 0u, SPLIT>;
-		if (fixed) return (const void*)k_step<true, false, PH_DEFAULT, SPLIT>;
-		return (const void*)k_step<true, false, 0u, SPLIT>;
+		if (dep) return (const void*)k_step<true, true>;
+		if (fixed) return (const void*)k_step<true, false, PH_DEFAULT>;
+		return (const void*)k_step<true, false>;
 	}
-	if (dep) return (const void*)k_step<false, true, 0u, SPLIT>;
-	if (fixed) return (const void*)k_step<false, false, PH_DEFAULT, SPLIT>;
-	return (const void*)k_step<false, false, 0u, SPLIT>;
-}
-
-static const void* step_kernel(const StepParams& p)
-{
-	return p.split ? step_kernel_for<true>(p) : step_kernel_for<false>(p);
+	if (dep) return (const void*)k_step<false, true>;
+	if (fixed) return (const void*)k_step<false, false, PH_DEFAULT>;
+	return (const void*)k_step<false, false>;
 }
 
 cudaError_t launch_step(const StepParams& p, uint32_t iteration, int grid, int block, cudaStream_t s)

@@ -251,9 +251,11 @@ def test_transport_deterministic_and_capacity_independent(inputs):
     outs = []
     spilled = []
     counters = []
-    # (pool capacity, threads per block, step mode: 0 fused, 1 split)
-    for cap, blk, mode in ((1 << 16, 256, 0), (1 << 12, 128, 0), (64, 64, 0), (1 << 16, 256, 1), (64, 64, 1)):
-        sim = nb.Simulation(g, [m], capacity=cap, seed=42, block_size=blk, step_mode=mode)
+    # (pool capacity, threads per block, leaf cells a walk takes per
+    # iteration before it continues in the next; 2^20: never cut)
+    for cap, blk, cells in ((1 << 16, 256, 1), (1 << 12, 128, 1), (64, 64, 1), (1 << 16, 256, 1 << 20),
+                            (64, 64, 1 << 20), (1 << 12, 128, 2), (64, 64, 3)):
+        sim = nb.Simulation(g, [m], capacity=cap, seed=42, block_size=blk, walk_cells=cells)
         sim.push(pri)
         sim.run()
         r = sim.flush_detected()
@@ -261,11 +263,13 @@ def test_transport_deterministic_and_capacity_independent(inputs):
         spilled.append(c["spilled"])
         counters.append({k: c[k] for k in ("flights", "boundary", "elastic", "inelastic", "spawned", "detected",
                                            "terminated", "primaries_started")})
+        # the slab's octree is shallow: walks continue at budgets of 1 and 2 cells
+        assert (c["walk_resumes"] == 0) if cells == 1 << 20 else (c["walk_resumes"] > 0 or cells > 2)
         outs.append(np.sort(r.view(np.dtype((np.void, 36))).ravel()).tobytes())
     assert all(o == outs[0] for o in outs[1:])
     assert all(c == counters[0] for c in counters[1:]), counters
     # the smallest pools must have parked secondaries in the overflow ring
-    assert spilled[2] > 0 and spilled[4] > 0
+    assert spilled[2] > 0 and spilled[4] > 0 and spilled[6] > 0
 
 
 def test_small_capacity_forces_many_refills(inputs):
