@@ -636,7 +636,8 @@ def run_case(args):
         from nebula_b200.tune_mixed_batch import load_mixed_batch
         with tempfile.TemporaryDirectory() as d:
             geoms, mats, jobs, _ = load_mixed_batch(d, scale=args.batch_scale)
-            b = nb.Batch(geoms, mats, capacity=args.capacity, block_size=args.block or 512, refill_threshold=0.5)
+            b = nb.Batch(geoms, mats, capacity=args.capacity, block_size=args.block or 512, refill_threshold=0.5,
+                         walk_cells=args.walk_cells)
             b.set_jobs(jobs)
             runs = []
             for r in range(args.repeat + 1):

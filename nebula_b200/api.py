@@ -265,7 +265,6 @@ class Simulation:
             self.deposit_grid_shape = (int(n[2]), int(n[1]), int(n[0]))
         p.stream = stream
         p.record_capacity = record_capacity
-        p.walk_cells = walk_cells
         self.params = p
         self.tally = tuple(tally)
         self.hist_bins = hist_bins
@@ -444,6 +443,7 @@ class Batch:
         p.max_events = max_events
         p.stream = stream
         p.record_capacity = record_capacity
+        p.walk_cells = walk_cells
         self.params = p
         self.geometries = list(geometries)
         self.materials = list(materials)
