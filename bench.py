@@ -364,11 +364,13 @@ def batched_vs_plain(args, dev, workdir):
     if os.path.exists(TUNED):
         best = autotune.load(TUNED)
         params = dict(capacity=int(best["capacity"]), block=int(best["block"]), threshold=float(best["threshold"]),
+                      walk_cells=int(best.get("walk_cells", 1)),
                       source="autotuner (nebula_b200/tuned/mixed_batch.json)")
     else:
-        params = dict(capacity=1 << 22, block=512, threshold=0.5, source="default")
+        params = dict(capacity=1 << 22, block=512, threshold=0.5, walk_cells=1, source="default")
     b = nb.Batch(geoms, mats, capacity=params["capacity"], block_size=params["block"],
-                 refill_threshold=params["threshold"], device=dev, record_capacity=1 << 24)
+                 refill_threshold=params["threshold"], device=dev, record_capacity=1 << 24,
+                 walk_cells=params["walk_cells"])
 
     # the batch's primaries laid end to end, as the caller holds them (the
     # plain arm holds one array per job)

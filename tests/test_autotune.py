@@ -5,15 +5,17 @@ from nebula_b200 import autotune
 def test_coordinate_descent_finds_separable_minimum():
     calls = []
 
-    def cost(cap, blk, thr):
-        calls.append((cap, blk, thr))
-        return 1.0 + abs(cap.bit_length() - 23) * 10 + abs(blk - 512) / 128 + abs(thr - 0.3) * 5
+    def cost(cap, blk, thr, cells):
+        calls.append((cap, blk, thr, cells))
+        return (1.0 + abs(cap.bit_length() - 23) * 10 + abs(blk - 512) / 128 + abs(thr - 0.3) * 5
+                + abs(cells - 2) * 3)
 
     best, table = autotune.tune_batch(None, None, [(0, 1, [0] * 10)], timer=cost)
-    assert (best["capacity"], best["block"], best["threshold"]) == (1 << 22, 512, 0.3)
+    assert (best["capacity"], best["block"], best["threshold"], best["walk_cells"]) == (1 << 22, 512, 0.3, 2)
     # every point timed once (cache), within the documented ranges
     assert len(calls) == len(set(calls)) == len(table)
-    assert all((1 << 18) <= c <= (1 << 24) and b in (128, 256, 512) and 0.1 <= t <= 1.0 for c, b, t in calls)
+    assert all((1 << 18) <= c <= (1 << 24) and b in (128, 256, 512) and 0.1 <= t <= 1.0 and w in (1, 2, 4)
+               for c, b, t, w in calls)
 
 
 def test_sample_keeps_every_job():
