@@ -82,6 +82,76 @@ __device__ __forceinline__ uint32_t warp_reserve5(uint32_t* counters, int q)
 	return base + (uint32_t)__popc(mq & lanemask_lt());
 }
 
+/* --------------------------------------------------------- streamed queue traffic */
+// Every queue entry is written once and read once, in the next iteration:
+// the event queues and the primaries stream through the 126 MB L2 at several
+// hundred MB per iteration.  They are loaded and stored with an evict-first
+// L2 policy and without allocating in L1, so that the caches keep the data
+// that is read over and over -- octree nodes, triangles, tables.  The loads
+// are ordered like the __ldcg loads they replace (the batched kernel reads
+// entries that other SMs wrote before its grid barrier).
+__device__ __forceinline__ uint64_t stream_policy()
+{
+	uint64_t p;
+	asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+	return p;
+}
+__device__ __forceinline__ float4 ld_stream(const float4* a)
+{
+	float4 v;
+	asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+		: "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(a), "l"(stream_policy()) : "memory");
+	return v;
+}
+__device__ __forceinline__ uint4 ld_stream(const uint4* a)
+{
+	uint4 v;
+	asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+		: "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(a), "l"(stream_policy()) : "memory");
+	return v;
+}
+__device__ __forceinline__ float2 ld_stream(const float2* a)
+{
+	float2 v;
+	asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;"
+		: "=f"(v.x), "=f"(v.y) : "l"(a), "l"(stream_policy()) : "memory");
+	return v;
+}
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* a)
+{
+	uint32_t v;
+	asm volatile("ld.global.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+		: "=r"(v) : "l"(a), "l"(stream_policy()) : "memory");
+	return v;
+}
+__device__ __forceinline__ float ld_stream(const float* a)
+{
+	float v;
+	asm volatile("ld.global.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;"
+		: "=f"(v) : "l"(a), "l"(stream_policy()) : "memory");
+	return v;
+}
+__device__ __forceinline__ void st_stream(float4* a, float4 v)
+{
+	asm volatile("st.global.L1::no_allocate.L2::cache_hint.v4.f32 [%0], {%1,%2,%3,%4}, %5;"
+		:: "l"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(stream_policy()) : "memory");
+}
+__device__ __forceinline__ void st_stream(uint4* a, uint4 v)
+{
+	asm volatile("st.global.L1::no_allocate.L2::cache_hint.v4.u32 [%0], {%1,%2,%3,%4}, %5;"
+		:: "l"(a), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "l"(stream_policy()) : "memory");
+}
+__device__ __forceinline__ void st_stream(float2* a, float2 v)
+{
+	asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f32 [%0], {%1,%2}, %3;"
+		:: "l"(a), "f"(v.x), "f"(v.y), "l"(stream_policy()) : "memory");
+}
+__device__ __forceinline__ void st_stream(uint32_t* a, uint32_t v)
+{
+	asm volatile("st.global.L1::no_allocate.L2::cache_hint.u32 [%0], %1, %2;"
+		:: "l"(a), "r"(v), "l"(stream_policy()) : "memory");
+}
+
 /* --------------------------------------------------------------- ray query */
 __global__ void k_ray_query(const DevGeometry g, const float* __restrict__ pos, const float* __restrict__ dir,
 	const float* __restrict__ dist, const int32_t* __restrict__ ignore_tri, const int32_t* __restrict__ ignore_mat,
@@ -224,8 +294,8 @@ struct FlightResume {
 
 __device__ __forceinline__ void load_resume(const Queue& q, uint32_t i, FlightResume& fr)
 {
-	const float4 w0 = __ldcg(q.w0 + i);
-	const uint4 w1 = __ldcg(q.w1 + i);
+	const float4 w0 = ld_stream(q.w0 + i);
+	const uint4 w1 = ld_stream(q.w1 + i);
 	fr.w.cx = w0.x; fr.w.cy = w0.y; fr.w.cz = w0.z; fr.w.to_go = w0.w;
 	fr.w.location = ((uint64_t)w1.y << 32) | w1.x;
 	fr.dist = __uint_as_float(w1.z);
@@ -236,9 +306,9 @@ __device__ __forceinline__ void load_resume(const Queue& q, uint32_t i, FlightRe
 
 __device__ __forceinline__ void store_resume(const Queue& q, uint32_t i, const FlightResume& fr)
 {
-	q.w0[i] = make_float4(fr.w.cx, fr.w.cy, fr.w.cz, fr.w.to_go);
-	q.w1[i] = make_uint4((uint32_t)fr.w.location, (uint32_t)(fr.w.location >> 32), __float_as_uint(fr.dist),
-		(uint32_t)fr.type | ((uint32_t)fr.hop << 2) | ((uint32_t)fr.w.steps << 4));
+	st_stream(q.w0 + i, make_float4(fr.w.cx, fr.w.cy, fr.w.cz, fr.w.to_go));
+	st_stream(q.w1 + i, make_uint4((uint32_t)fr.w.location, (uint32_t)(fr.w.location >> 32), __float_as_uint(fr.dist),
+		(uint32_t)fr.type | ((uint32_t)fr.hop << 2) | ((uint32_t)fr.w.steps << 4)));
 }
 
 // Free flight(s) from the electron's current state: domain and energy cut,
@@ -339,10 +409,10 @@ __device__ __forceinline__ int free_flight(const StepParams& P, const RunView& r
 __device__ __forceinline__ void store_electron(const Queue& q, uint32_t slot, const Electron& p, int mat, int last_tri,
 	uint32_t tag, uint32_t event, uint64_t lineage)
 {
-	q.a[slot] = make_float4(p.pos.x, p.pos.y, p.pos.z, p.E);
-	q.b[slot] = make_float4(p.dir.x, p.dir.y, p.dir.z, __int_as_float(mat));
-	q.c[slot] = make_uint4((uint32_t)last_tri, tag, event, (uint32_t)lineage);
-	q.d[slot] = (uint32_t)(lineage >> 32);
+	st_stream(q.a + slot, make_float4(p.pos.x, p.pos.y, p.pos.z, p.E));
+	st_stream(q.b + slot, make_float4(p.dir.x, p.dir.y, p.dir.z, __int_as_float(mat)));
+	st_stream(q.c + slot, make_uint4((uint32_t)last_tri, tag, event, (uint32_t)lineage));
+	st_stream(q.d + slot, (uint32_t)(lineage >> 32));
 }
 
 // Loads of data written during the same launch by other SMs bypass L1
@@ -505,22 +575,22 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		FlightResume fr;
 		if (kind == K_RING || (kind >= 0 && kind < N_QUEUES)) {
 			const Queue& q = kind == K_RING ? P.spill : qin[kind];
-			const float4 a = __ldcg(q.a + qi), b = __ldcg(q.b + qi);
-			const uint4 c = __ldcg(q.c + qi);
+			const float4 a = ld_stream(q.a + qi), b = ld_stream(q.b + qi);
+			const uint4 c = ld_stream(q.c + qi);
 			p.pos = v3(a.x, a.y, a.z); p.E = a.w;
 			p.dir = v3(b.x, b.y, b.z); mat = __float_as_int(b.w);
 			last_tri = (int)c.x; tag = c.y; event = c.z;
-			lineage = ((uint64_t)__ldcg(q.d + qi) << 32) | c.w;
+			lineage = ((uint64_t)ld_stream(q.d + qi) << 32) | c.w;
 			if (ADJ) {
-				const float4 s = __ldcg(q.s + qi);
-				const float2 s2 = __ldcg(q.s2 + qi);
+				const float4 s = ld_stream(q.s + qi);
+				const float2 s2 = ld_stream(q.s2 + qi);
 				sc[0] = s.x; sc[1] = s.y; sc[2] = s.z; sc[3] = s.w; sc[4] = s2.x; sc[5] = s2.y;
 			}
 		} else if (kind == K_PRIMARY) {
 			const Record36* r = P.primaries + qi;
-			p.pos = v3(r->x, r->y, r->z);
-			p.dir = v3(r->dx, r->dy, r->dz);
-			p.E = r->E;
+			p.pos = v3(ld_stream(&r->x), ld_stream(&r->y), ld_stream(&r->z));
+			p.dir = v3(ld_stream(&r->dx), ld_stream(&r->dy), ld_stream(&r->dz));
+			p.E = ld_stream(&r->E);
 			if (BATCH) {
 				const uint32_t j = job_of(B, qi);
 				tag = (j << 24) | (qi - __ldg(&B.jobs[j].first));
@@ -695,8 +765,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			if (dst) {
 				store_electron(*dst, at, se, mat, -1, tag, 0u, se_lineage);
 				if (ADJ) {
-					dst->s[at] = make_float4(sc[0], sc[1], sc[2], sc[3]);
-					dst->s2[at] = make_float2(sc[4], sc[5]);
+					st_stream(dst->s + at, make_float4(sc[0], sc[1], sc[2], sc[3]));
+					st_stream(dst->s2 + at, make_float2(sc[4], sc[5]));
 				}
 			}
 		}
@@ -719,8 +789,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 				if (qtype == t && slot < P.qcap) {
 					store_electron(qout[t], slot, p, mat, last_tri, tag, event, lineage);
 					if (ADJ) {
-						qout[t].s[slot] = make_float4(sc[0], sc[1], sc[2], sc[3]);
-						qout[t].s2[slot] = make_float2(sc[4], sc[5]);
+						st_stream(qout[t].s + slot, make_float4(sc[0], sc[1], sc[2], sc[3]));
+						st_stream(qout[t].s2 + slot, make_float2(sc[4], sc[5]));
 					}
 					if (t == EV_WALK)
 						store_resume(qout[t], slot, fr);
