@@ -243,10 +243,12 @@ struct nbl_sim {
 		return (int64_t)(queued(c) + spill_occupancy(c) + (n_pri - c[SLOT_CURSOR]));
 	}
 
+	// electrons in the queues of a control slot (the flight queue's count
+	// also counts the tickets of secondaries that went to the spill ring)
 	static uint64_t queued(const uint32_t* c)
 	{
 		uint64_t n = 0;
-		for (int q = 0; q < N_QUEUES; ++q) n += c[q];
+		for (int q = 0; q < N_QUEUES; ++q) n += q == EV_NEW ? std::min(c[q], c[SLOT_NEW_BUDGET]) : c[q];
 		return n;
 	}
 

@@ -29,11 +29,13 @@ enum : int {
 };
 
 // Per-iteration control words, three rotating slots of 16 words:
-// [queue counts x N_QUEUES, primary cursor, secondary tickets, spill head,
+// [queue counts x N_QUEUES, primary cursor, secondary budget, spill head,
 //  spill tail at iteration start, spill pushes this iteration, work, pad].
+// The flight queue's count also hands out the secondaries' tickets, so it
+// can exceed the entries written: those are min(count, budget).
 constexpr int SLOT_WORDS = 16;
 constexpr int SLOT_CURSOR = N_QUEUES;
-constexpr int SLOT_TICKETS = N_QUEUES + 1;
+constexpr int SLOT_NEW_BUDGET = N_QUEUES + 1;
 constexpr int SLOT_SPILL_HEAD = N_QUEUES + 2;
 constexpr int SLOT_SPILL_TAIL = N_QUEUES + 3;
 constexpr int SLOT_SPILL_PUSHED = N_QUEUES + 4;

@@ -299,7 +299,7 @@ extern "C" nbl_status nbl_run_noalloc(const nbl_geometry* g, nbl_material* const
 			cuda_ok(cudaStreamSynchronize(s), "transport");
 			uint64_t active = (uint32_t)(ctrl[SLOT_SPILL_TAIL] + ctrl[SLOT_SPILL_PUSHED] - ctrl[SLOT_SPILL_HEAD]);
 			for (int q = 0; q < N_QUEUES; ++q)
-				active += ctrl[q];
+				active += q == EV_NEW ? std::min(ctrl[q], ctrl[SLOT_NEW_BUDGET]) : ctrl[q];
 			done = active == 0 && ctrl[SLOT_CURSOR] == (uint32_t)n_primaries;
 			if (!done) {
 				stalled = flights == last_flights ? stalled + 1 : 0;

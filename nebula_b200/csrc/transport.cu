@@ -498,7 +498,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 	// counts are clamped to the queue capacity (the secondary budget below
 	// keeps them there; the clamp makes an out-of-range read impossible)
 	const uint32_t n0 = min(ld_ctrl(cr + 0), P.qcap), n1 = min(ld_ctrl(cr + 1), P.qcap);
-	const uint32_t n2 = min(ld_ctrl(cr + 2), P.qcap), n3 = min(ld_ctrl(cr + 3), P.qcap);
+	const uint32_t n2 = min(ld_ctrl(cr + 2), P.qcap);
+	const uint32_t n3 = min(min(ld_ctrl(cr + EV_NEW), ld_ctrl(cr + SLOT_NEW_BUDGET)), P.qcap);
 	const uint32_t n4 = min(ld_ctrl(cr + 4), P.qcap);
 	const uint32_t cursor = ld_ctrl(cr + SLOT_CURSOR);
 	const uint32_t e1 = n0 + n1, e2 = e1 + n2, e2n = e2 + n3, active = e2n + n4;
@@ -527,6 +528,7 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		cw[SLOT_CURSOR] = cursor + nr;
 		cw[SLOT_SPILL_HEAD] = sp_head + n_drain;
 		cw[SLOT_SPILL_TAIL] = sp_tail;
+		cw[SLOT_NEW_BUDGET] = se_budget;
 		uint32_t* cz = P.ctrl + zs * SLOT_WORDS;
 #pragma unroll
 		for (int k = 0; k < SLOT_WORDS; ++k)
@@ -744,10 +746,13 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 				lc.add(CNT_TERMINATED);
 			}
 		}
-		const uint32_t ticket = warp_reserve(cw + SLOT_TICKETS, spawn);
-		const bool queued = spawn && ticket < se_budget;
+		// The flight queue's counter hands out the tickets: the first
+		// se_budget secondaries are queued, later ones go to the spill ring
+		// (their slots stay unwritten; the next iteration reads at most
+		// se_budget entries).
+		const uint32_t sslot = warp_reserve(cw + EV_NEW, spawn);
+		const bool queued = spawn && sslot < se_budget;
 		const bool spilled = spawn && !queued;
-		const uint32_t sslot = warp_reserve(cw + EV_NEW, queued);
 		const uint32_t pslot = warp_reserve(cw + SLOT_SPILL_PUSHED, spilled);
 		if (queued || spilled) {
 			const Queue* dst = nullptr;
@@ -779,6 +784,11 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		if (kind >= 0 && status != ST_DETECTED && qtype < 0)
 			lc.add(CNT_TERMINATED);
 		{
+			// the warp's next chunk is claimed (lane 5) together with the
+			// queue slots (lanes 0-4): one atomic round trip for both
+			uint32_t next = 0u;
+			if (lane == 5u)
+				next = atomicAdd(work, 32u);
 			const uint32_t slot = warp_reserve5(cw, qtype);
 			if (qtype >= 0 && slot >= P.qcap)
 				lc.add(CNT_QUEUE_OVERFLOW);
@@ -796,9 +806,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 						store_resume(qout[t], slot, fr);
 				}
 			}
+			base = __shfl_sync(0xFFFFFFFFu, next, 5);
 		}
-		if (lane == 0u) base = atomicAdd(work, 32u);
-		base = __shfl_sync(0xFFFFFFFFu, base, 0);
 	}
 	return true;
 }
