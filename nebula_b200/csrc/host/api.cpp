@@ -200,10 +200,11 @@ struct nbl_sim {
 			read_ctrl(c);
 			// records stay on the device until the buffer could not take two
 			// more graphs' worth (the most one graph has added so far, at
-			// least 1/8 of the buffer); then they are parked on the host
+			// least a quarter of the buffer: a run's early graphs detect less
+			// than its later ones); then they are parked on the host
 			const uint32_t ndet = pinned_ctrl[SLOT_WORDS];
 			record_growth = std::max(record_growth, ndet >= records_seen ? ndet - records_seen : ndet);
-			const uint64_t reserve = std::max<uint64_t>(2ull * record_growth, sp.det_cap / 8);
+			const uint64_t reserve = std::max<uint64_t>(2ull * record_growth, sp.det_cap / 4);
 			if (!sink && (uint64_t)ndet + reserve > sp.det_cap) {
 				drain_to_host(ndet);
 				records_seen = 0;
