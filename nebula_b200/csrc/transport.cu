@@ -431,6 +431,78 @@ __device__ __forceinline__ uint32_t job_of(const BatchParams& B, uint32_t g)
 	return (uint32_t)lo;
 }
 
+// The six adjoint scores of an electron, by value.
+struct Scores {
+	float v[6];
+};
+
+// Detection output of the lanes of a warp that detected an electron
+// (`det`): per-pixel SE / BSE tallies (with the detector acceptance cone),
+// adjoint gradient sums, the energy histogram and the 36-byte record
+// (gpu_main.cu:216-223).  Called by every lane of a warp in which any lane
+// detected; kept out of line so that the hot loop's instructions stay few.
+template<bool ADJ, bool BATCH>
+__device__ __noinline__ void detection_output(const StepParams* Pp, const BatchParams* Bp, bool det, Electron p,
+	uint32_t rec_index, uint32_t job, PhiloxKey key, uint32_t stream_tag, Scores sc, bool wshift, uint32_t* s_counters)
+{
+	const StepParams& P = *Pp;
+	LocalCounters lc{ s_counters };
+	if (det) {
+		lc.add(CNT_DETECTED);
+		const Tallies& T = P.tal;
+		if (BATCH) {
+			atomicAdd((p.E < 50.0f ? Bp->job_se : Bp->job_bse) + job, 1ull);
+		} else {
+			const Record36* pr = P.primaries + rec_index;
+			const int px = pr->px, py = pr->py;
+			bool seen = true;
+			if (T.filter) {
+				// detector acceptance: polar angle of the detected direction to +z
+				const float c = fdf(p.dir.z, __fsqrt_rn(vmag2(p.dir)));
+				seen = c >= T.cos_min && c <= T.cos_max;
+			}
+			if (seen && T.se_img && px >= 0 && py >= 0 && px < T.nx && py < T.ny) {
+				const size_t pix = (size_t)py * T.nx + px;
+				atomicAdd((p.E < 50.0f ? T.se_img : T.bse_img) + pix, 1u);
+				if (ADJ && T.grad_se) {
+					double* g = (p.E < 50.0f ? T.grad_se : T.grad_bse) + pix * 6;
+#pragma unroll
+					for (int k = 0; k < 6; ++k)
+						if (k % 3 != 2 || !wshift)
+							atomicAdd(g + k, (double)sc.v[k]);
+				}
+				if (T.wsign_se) {
+					int32_t* w = (p.E < 50.0f ? T.wsign_se : T.wsign_bse) + pix * 2;
+					atomicAdd(w, (int32_t)wsign(key, stream_tag, 0));
+					atomicAdd(w + 1, (int32_t)wsign(key, stream_tag, 1));
+				}
+			}
+		}
+		if (T.hist && p.E >= 0.0f && p.E < T.hist_emax) {
+			int bin = (int)(p.E / T.hist_emax * (float)T.n_bins);
+			bin = bin < T.n_bins ? bin : T.n_bins - 1;
+			atomicAdd(T.hist + bin, 1u);
+		}
+	}
+	if (P.detected) {
+		const uint32_t rslot = warp_reserve(P.n_detected, det);
+		if (det) {
+			if (rslot < P.det_cap) {
+				Record36 rec;
+				const Record36* pr = P.primaries + rec_index;
+				rec.x = p.pos.x; rec.y = p.pos.y; rec.z = p.pos.z;
+				rec.dx = p.dir.x; rec.dy = p.dir.y; rec.dz = p.dir.z; rec.E = p.E;
+				rec.px = pr->px; rec.py = pr->py;
+				P.detected[rslot] = rec;
+				if (BATCH && P.det_job)
+					P.det_job[rslot] = (uint8_t)job;
+			} else {
+				lc.add(CNT_RECORD_OVERFLOW);
+			}
+		}
+	}
+}
+
 // One wavefront iteration over the index space
 //   [boundary | elastic | inelastic | new secondaries | drained ring | primaries].
 // Returns false when there was no work at all (the run is finished); every
@@ -671,61 +743,14 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			deposit(P, (kind == EV_ELASTIC || kind == EV_INELASTIC) && p.E != e_before, p, e_before,
 				P.primaries + rec_index, s_lane + (threadIdx.x & ~31u), lc);
 
-		// detection output: record + tallies
-		if (status == ST_DETECTED) {
-			lc.add(CNT_DETECTED);
-			const Tallies& T = P.tal;
-			if (BATCH) {
-				atomicAdd((p.E < 50.0f ? B.job_se : B.job_bse) + job, 1ull);
-			} else {
-				const Record36* pr = P.primaries + rec_index;
-				const int px = pr->px, py = pr->py;
-				bool seen = true;
-				if (T.filter) {
-					// detector acceptance: polar angle of the detected direction to +z
-					const float c = fdf(p.dir.z, __fsqrt_rn(vmag2(p.dir)));
-					seen = c >= T.cos_min && c <= T.cos_max;
-				}
-				if (seen && T.se_img && px >= 0 && py >= 0 && px < T.nx && py < T.ny) {
-					const size_t pix = (size_t)py * T.nx + px;
-					atomicAdd((p.E < 50.0f ? T.se_img : T.bse_img) + pix, 1u);
-					if (ADJ && T.grad_se) {
-						double* g = (p.E < 50.0f ? T.grad_se : T.grad_bse) + pix * 6;
+		// detection output: record + tallies (out of line: a warp has a
+		// detection in a small fraction of its chunks)
+		if (__any_sync(0xFFFFFFFFu, status == ST_DETECTED)) {
+			Scores scs;
 #pragma unroll
-						for (int k = 0; k < 6; ++k)
-							if (k % 3 != 2 || !wshift)
-								atomicAdd(g + k, (double)sc[k]);
-					}
-					if (T.wsign_se) {
-						int32_t* w = (p.E < 50.0f ? T.wsign_se : T.wsign_bse) + pix * 2;
-						atomicAdd(w, (int32_t)wsign(rv.key, stream_tag, 0));
-						atomicAdd(w + 1, (int32_t)wsign(rv.key, stream_tag, 1));
-					}
-				}
-			}
-			if (T.hist && p.E >= 0.0f && p.E < T.hist_emax) {
-				int bin = (int)(p.E / T.hist_emax * (float)T.n_bins);
-				bin = bin < T.n_bins ? bin : T.n_bins - 1;
-				atomicAdd(T.hist + bin, 1u);
-			}
-		}
-		if (P.detected) {
-			const bool det = status == ST_DETECTED;
-			const uint32_t rslot = warp_reserve(P.n_detected, det);
-			if (det) {
-				if (rslot < P.det_cap) {
-					Record36 rec;
-					const Record36* pr = P.primaries + rec_index;
-					rec.x = p.pos.x; rec.y = p.pos.y; rec.z = p.pos.z;
-					rec.dx = p.dir.x; rec.dy = p.dir.y; rec.dz = p.dir.z; rec.E = p.E;
-					rec.px = pr->px; rec.py = pr->py;
-					P.detected[rslot] = rec;
-					if (BATCH && P.det_job)
-						P.det_job[rslot] = (uint8_t)job;
-				} else {
-					lc.add(CNT_RECORD_OVERFLOW);
-				}
-			}
+			for (int k = 0; k < 6; ++k) scs.v[k] = ADJ ? sc[k] : 0.0f;
+			detection_output<ADJ, BATCH>(&P, BATCH ? &B : nullptr, status == ST_DETECTED, p, rec_index, job, rv.key,
+				stream_tag, scs, wshift, lc.c);
 		}
 
 		// secondary: inherits material, tag and the parent's scores; its
@@ -827,7 +852,7 @@ __device__ __forceinline__ void flush_counters(const StepParams& P, uint32_t* s_
 // none of their code).  PHC: nonzero = the physics selection fixed at
 // compile time (PH_DEFAULT only).
 template<bool ADJ, bool DEP, uint32_t PHC = 0u>
-__global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const StepParams P, uint32_t it)
+__global__ void __launch_bounds__(256, NBL_STEP_MIN_BLOCKS) k_step(const __grid_constant__ StepParams P, uint32_t it)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
 	__shared__ float s_lane[DEP ? 256 : 1];
@@ -878,7 +903,8 @@ __device__ __forceinline__ bool grid_barrier(const BatchParams& B)
 // boundary; it ends when an iteration finds no work (all blocks see the same
 // control words) or after max_iterations (error word set).
 template<bool ADJ, uint32_t PHC = 0u>
-__global__ void __launch_bounds__(512, 2) k_batch(const StepParams P, const BatchParams B)
+__global__ void __launch_bounds__(512, 2) k_batch(const __grid_constant__ StepParams P,
+	const __grid_constant__ BatchParams B)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
 	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
