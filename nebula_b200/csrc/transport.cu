@@ -3,14 +3,19 @@
 // The plain method is a wavefront: every iteration is ONE launch of k_step,
 // which walks a combined index space
 //
-//     [ boundary | elastic | inelastic | new secondaries | new primaries ]
+//     [ boundary | elastic | inelastic | new secondaries | continued walks |
+//       drained spill ring | new primaries ]
 //
-// where the first four segments are this iteration's event queues and the
-// last is the refill from the device-resident primary buffer (filled so that
-// at most `capacity` electrons are in flight, at most `ramp` per iteration).  Each item performs the
-// interaction that ended its previous free flight, then its next free flight
-// (free-path sampling + octree walk), and is appended to the next
-// iteration's queue for the event that flight ended in.  Queues are
+// where the first five segments are this iteration's queues, then the
+// secondaries parked in the overflow ring, then the refill from the
+// device-resident primary buffer (filled so that at most `capacity`
+// electrons are in flight, at most `ramp` per iteration).  Each item performs
+// the interaction that ended its previous free flight, then its next free
+// flight (free-path sampling + octree walk), and is appended to the next
+// iteration's queue for the event that flight ended in.  A walk stops after
+// `walk_cells` leaf cells (default 1); an unfinished one is appended to the
+// continued-walk queue with its exact state and goes on in the next
+// iteration, so a warp never waits on its lane with the longest walk.  Queues are
 // structure-of-arrays and double-buffered; appends are warp-aggregated
 // (one ballot and one atomic per warp and queue), so each queue segment a
 // warp reads or writes is contiguous and coalesced.  Sorting items by event
