@@ -302,13 +302,15 @@ nbl_status nbl_sim_set_seed(nbl_sim* s, uint64_t seed);
 nbl_status nbl_sim_kernel_ms(nbl_sim* s, double* ms);
 void nbl_sim_destroy(nbl_sim* s);
 
-/* Record sink: page-locked host memory (mapped into the device's address
- * space; pageable memory is page-locked here) that the transport kernel writes
- * the detected records of later runs into directly, as they are produced --
- * no copy after the run.  Records of a run start at host[0] after a reset, in
- * the order nbl_sim_drain_detected would return them; a run with more records
- * than `capacity` fails with NBL_ERR_POOL_OVERFLOW.  capacity 0 removes the
- * sink (records go to the device buffer again).  No counterpart in the
+/* Record sink: page-locked host memory (pageable memory is page-locked here)
+ * that receives the detected records of later runs while they run: the
+ * records each graph of iterations adds to the device buffer are copied into
+ * it on a copy stream while the next graph runs, so when nbl_sim_run returns
+ * only the last graph's copy has been waited for.  Records of a run start at
+ * host[0] after a reset, in the order nbl_sim_drain_detected would return
+ * them; a run with more records than `capacity` fails with
+ * NBL_ERR_POOL_OVERFLOW.  capacity 0 removes the sink (records stay in the
+ * device buffer for nbl_sim_drain_detected again).  No counterpart in the
  * reference (its flush_buffered copies the whole pool per frame). */
 nbl_status nbl_sim_set_record_sink(nbl_sim* s, nbl_record* host, int64_t capacity);
 /* Records in the sink so far. */

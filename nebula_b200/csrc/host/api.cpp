@@ -90,27 +90,53 @@ struct nbl_sim {
 	uint32_t record_growth = 0;             // most records one graph has added
 	uint32_t* pinned_ctrl = nullptr;
 
-	// Record sink: page-locked host memory the step kernel writes the detected
-	// records into directly (over the bus, as they are produced), so a run's
-	// output needs no copy after it.
+	// Record sink: page-locked host memory that receives a run's detected
+	// records while it runs.  The kernel appends them to the device buffer;
+	// after each graph the records that graph added are copied into the sink
+	// on a copy stream while the next graph runs, so only the last graph's
+	// copy is left when the run ends (the kernel's own 36-byte stores stay in
+	// device memory instead of crossing the bus one by one).
 	nbl_record* sink = nullptr;
-	void* sink_dev = nullptr;               // its device-side address
 	int64_t sink_cap = 0;
 	bool sink_registered = false;           // page-locked by this library
 	uint32_t dev_det_cap = 0;               // capacity of the device record buffer
+	cudaStream_t cstream = nullptr;         // the copies into the sink
+	uint64_t sink_fill = 0;                 // records copied (or on their way) into the sink
+	uint32_t dev_copied = 0;                // of the device buffer, records already sent to the sink
+	bool sink_overflow = false;             // a run had more records than the sink holds
 
 	void release_sink()
 	{
+		if (cstream) cudaStreamSynchronize(cstream);
 		if (sink_registered && sink) cudaHostUnregister(sink);
 		sink_registered = false;
 		sink = nullptr;
-		sink_dev = nullptr;
 		sink_cap = 0;
+	}
+
+	// Send the device buffer's records [dev_copied, ndet) to the sink (they
+	// were written by graphs that have completed).
+	void sink_copy(uint32_t ndet)
+	{
+		ndet = std::min(ndet, sp.det_cap);
+		if (ndet <= dev_copied)
+			return;
+		uint64_t n = ndet - dev_copied;
+		if (sink_fill + n > (uint64_t)sink_cap) {
+			sink_overflow = true;
+			n = sink_fill < (uint64_t)sink_cap ? (uint64_t)sink_cap - sink_fill : 0;
+		}
+		if (n)
+			CU(cudaMemcpyAsync(sink + sink_fill, detected.as<nbl_record>() + dev_copied, (size_t)n * sizeof(nbl_record),
+				cudaMemcpyDeviceToHost, cstream));
+		sink_fill += n;
+		dev_copied = ndet;
 	}
 
 	~nbl_sim()
 	{
 		release_sink();
+		if (cstream) cudaStreamDestroy(cstream);
 		if (graph) cudaGraphExecDestroy(graph);
 		if (ev0) cudaEventDestroy(ev0);
 		if (ev1) cudaEventDestroy(ev1);
@@ -205,7 +231,19 @@ struct nbl_sim {
 			const uint32_t ndet = pinned_ctrl[SLOT_WORDS];
 			record_growth = std::max(record_growth, ndet >= records_seen ? ndet - records_seen : ndet);
 			const uint64_t reserve = std::max<uint64_t>(2ull * record_growth, sp.det_cap / 4);
-			if (!sink && (uint64_t)ndet + reserve > sp.det_cap) {
+			if (sink) {
+				sink_copy(ndet);
+				if ((uint64_t)ndet + reserve > sp.det_cap) {
+					// the buffer is reused from its start once its records
+					// are in the sink
+					CU(cudaStreamSynchronize(cstream));
+					CU(cudaMemsetAsync(n_detected.p, 0, sizeof(uint32_t), stream));
+					dev_copied = 0;
+					records_seen = 0;
+				} else {
+					records_seen = ndet;
+				}
+			} else if ((uint64_t)ndet + reserve > sp.det_cap) {
 				drain_to_host(ndet);
 				records_seen = 0;
 			} else {
@@ -267,8 +305,18 @@ struct nbl_sim {
 		return c[CNT_FLIGHTS] + c[CNT_RESUMED];
 	}
 
+	// the copies into the sink of the graphs run so far have landed
+	void sink_wait()
+	{
+		if (sink)
+			CU(cudaStreamSynchronize(cstream));
+	}
+
 	void check_errors()
 	{
+		if (sink_overflow)
+			throw Error(NBL_ERR_POOL_OVERFLOW, "the record sink holds " + std::to_string(sink_cap) +
+				" records, the run detected more; pass a larger sink");
 		unsigned long long cnt[N_COUNTERS];
 		CU(cudaMemcpyAsync(cnt, counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
 		CU(cudaStreamSynchronize(stream));
@@ -307,6 +355,9 @@ struct nbl_sim {
 		kernel_ms = 0;
 		host_records.clear();
 		records_seen = 0;
+		sink_fill = 0;
+		dev_copied = 0;
+		sink_overflow = false;
 	}
 
 	void ensure_primary_capacity(uint64_t need)
@@ -865,6 +916,7 @@ nbl_status nbl_sim_step(nbl_sim* s, uint32_t iterations, int64_t* running)
 		set_device(s->device);
 		const uint64_t graphs = (iterations + s->graph_iters - 1) / s->graph_iters;
 		const int64_t r = s->advance(std::max<uint64_t>(graphs, 1));
+		s->sink_wait();
 		if (running) *running = r;
 		s->check_errors();
 	});
@@ -884,6 +936,7 @@ nbl_status nbl_sim_run(nbl_sim* s)
 		const uint64_t bound = ((uint64_t)s->sp.max_events + 1) * 64 + s->n_pri + 16;
 		const uint64_t max_graphs = bound / s->graph_iters + 2;
 		const int64_t left = s->advance(max_graphs);
+		s->sink_wait();
 		s->check_errors();
 		if (left != 0)
 			throw Error(NBL_ERR_BUDGET_EXCEEDED, "run did not finish within its iteration bound");
@@ -899,28 +952,27 @@ nbl_status nbl_sim_set_record_sink(nbl_sim* s, nbl_record* host, int64_t capacit
 		CU(cudaStreamSynchronize(s->stream));
 		s->release_sink();
 		if (capacity > 0) {
-			void* dev = nullptr;
 			cudaPointerAttributes a{};
-			if (cudaPointerGetAttributes(&a, host) == cudaSuccess && a.type == cudaMemoryTypeHost && a.devicePointer) {
-				dev = a.devicePointer;
-			} else {
+			if (!(cudaPointerGetAttributes(&a, host) == cudaSuccess && a.type == cudaMemoryTypeHost)) {
 				cudaGetLastError();
-				const cudaError_t e = cudaHostRegister(host, (size_t)capacity * sizeof(nbl_record),
-					cudaHostRegisterMapped);
+				const cudaError_t e = cudaHostRegister(host, (size_t)capacity * sizeof(nbl_record), cudaHostRegisterDefault);
 				if (e != cudaSuccess) {
 					cudaGetLastError();
-					throw Error(NBL_ERR_INVALID_ARG, "the record sink could not be page-locked and mapped");
+					throw Error(NBL_ERR_INVALID_ARG, "the record sink could not be page-locked");
 				}
 				s->sink_registered = true;
-				CU(cudaHostGetDevicePointer(&dev, host, 0));
 			}
+			if (!s->cstream)
+				CU(cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking));
 			s->sink = host;
-			s->sink_dev = dev;
 			s->sink_cap = capacity;
 		}
-		// records of later runs go to the sink (or back to the device buffer)
-		s->sp.detected = s->sink ? static_cast<Record36*>(s->sink_dev) : s->detected.as<Record36>();
-		s->sp.det_cap = s->sink ? (uint32_t)s->sink_cap : s->dev_det_cap;
+		// records of later runs go to the device buffer either way
+		s->sp.detected = s->detected.as<Record36>();
+		s->sp.det_cap = s->dev_det_cap;
+		s->sink_fill = 0;
+		s->dev_copied = 0;
+		s->sink_overflow = false;
 		s->graph_dirty = true;
 		CU(cudaMemsetAsync(s->n_detected.p, 0, sizeof(uint32_t), s->stream));
 		CU(cudaStreamSynchronize(s->stream));
@@ -933,12 +985,8 @@ nbl_status nbl_sim_sink_count(nbl_sim* s, int64_t* n)
 	return guard([&] {
 		require(s && n, "null argument");
 		set_device(s->device);
-		uint32_t d = 0;
-		if (s->sink) {
-			CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
-			CU(cudaStreamSynchronize(s->stream));
-		}
-		*n = std::min<int64_t>(d, s->sink_cap);
+		s->sink_wait();
+		*n = s->sink ? (int64_t)s->sink_fill : 0;
 	});
 }
 
@@ -950,7 +998,8 @@ nbl_status nbl_sim_detected_count(nbl_sim* s, int64_t* n)
 		uint32_t d = 0;
 		CU(cudaMemcpyAsync(&d, s->n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
 		CU(cudaStreamSynchronize(s->stream));
-		*n = (int64_t)s->host_records.size() + std::min(d, s->sp.det_cap);
+		// with a record sink the device buffer's records are the sink's
+		*n = (int64_t)s->host_records.size() + (s->sink ? 0u : std::min(d, s->sp.det_cap));
 	});
 }
 
@@ -1027,7 +1076,7 @@ nbl_status nbl_sim_counters(nbl_sim* s, nbl_counters* out)
 		out->spilled = c[CNT_SPILLED];
 		out->iterations = s->iteration;
 		out->primaries_total = s->n_pri;
-		out->records_pending = s->host_records.size() + std::min(d, s->sp.det_cap);
+		out->records_pending = s->host_records.size() + (s->sink ? 0u : std::min(d, s->sp.det_cap));
 		out->deposits = c[CNT_DEPOSITS];
 		out->deposit_overflow = c[CNT_DEPOSIT_OVERFLOW];
 		uint32_t nd = 0;
