@@ -11,9 +11,10 @@ and its full secondary cascade.
 value: primaries/s with the primary records already in HBM when the timed
        region starts (a device-to-device push, then the run).
 e2e:   the same through the public API from pinned host records: host->device
-       copy of the primaries, the run (the kernel writes every detected
-       36-byte record into a pinned host buffer as it finds it), and the
-       device->host copy of the tallies, all inside the timed region.
+       copy of the primaries (streamed in chunks while the run starts), the
+       run (every detected 36-byte record copied into a pinned host buffer
+       while the run goes), and the device->host copy of the tallies, all
+       inside the timed region.
 
 The same line also carries: the mixed 64-job batch, batched kernel against
 the plain kernel job after job (``batched``); the seed-replay adjoint against
@@ -571,8 +572,8 @@ def rough_lines(args, dev, workdir):
     512 x 512 pixel scan x 200 primaries at 300 eV (52.4 M primaries, built in
     device memory).  Reports the host octree build time (all host threads)
     and primaries/s over the run's wall time, every detected record delivered
-    to page-locked host memory (the record sink, written by the kernel as it
-    detects) and the per-pixel tallies on the device."""
+    to page-locked host memory (the record sink, copied there graph by graph
+    while the run goes) and the per-pixel tallies on the device."""
     import torch
     import nebula_b200 as nb
     from nebula_b200.synth import geometry, materials, nmat
@@ -621,7 +622,7 @@ def rough_lines(args, dev, workdir):
                         % (len(tris), n),
             "value": n / t, "unit": "primaries/s", "seconds": t, "events_per_primary": flights / n,
             "se_yield": float(se.sum()) / n, "bse_yield": float(bse.sum()) / n,
-            "records": n_rec, "records_to": "page-locked host memory, written by the kernel during the run",
+            "records": n_rec, "records_to": "page-locked host memory, copied graph by graph during the run",
             "octree_words": int(info["n_octree"]), "octree_build_seconds": t_build,
             "octree_build_threads": os.cpu_count(), "mesh_generation_seconds": t_gen}
 
@@ -794,11 +795,15 @@ def main():
             sim.push_device(pri_dev.data_ptr(), n_pri)
             sim.run()
 
+        pri_host_view = np.frombuffer(pri_host.numpy(), dtype=nb.PRI_DTYPE)
+
         def step_e2e():
-            # the kernel writes the detected records straight into the pinned
-            # host buffer as it finds them (the record sink)
+            # the primaries stream in from the pinned host buffer while the
+            # run starts (each admitted once its chunk has landed); the
+            # detected records are copied into the pinned host sink while
+            # the run goes
             sim.reset()
-            sim.push(np.frombuffer(pri_host.numpy(), dtype=nb.PRI_DTYPE))
+            sim.push_streamed(pri_host_view)
             sim.run()
             rec = sim.sink_records()
             tal = sim.tallies()

@@ -268,6 +268,14 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 nbl_status nbl_sim_push_primaries(nbl_sim* s, const nbl_record* recs, int64_t n);
 /* Same from device memory (records already resident in HBM). */
 nbl_status nbl_sim_push_primaries_device(nbl_sim* s, const void* d_recs, int64_t n);
+/* The same from page-locked host memory without waiting for the copy: the
+ * records are copied in chunks on a copy stream, and the next run admits
+ * each primary once its chunk has landed, so the copy overlaps the
+ * transport (the reference streams its input buffer frame by frame,
+ * gpu_driver.inl:215-254).  `recs` must stay valid and unchanged until the
+ * next nbl_sim_run / nbl_sim_step returns or nbl_sim_reset; pageable memory
+ * is rejected (use nbl_sim_push_primaries). */
+nbl_status nbl_sim_push_primaries_streamed(nbl_sim* s, const nbl_record* recs, int64_t n);
 /* Index of the first primary pushed within a larger scan (default 0).  A
  * primary's random numbers are keyed by the seed and this index, so a scan
  * resumed at primary k (first = k, pushing primaries k..) or split over

@@ -132,6 +132,7 @@ _DECLS = [
                                  C.POINTER(C.c_void_p)]),
     ("nbl_sim_push_primaries", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("nbl_sim_push_primaries_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
+    ("nbl_sim_push_primaries_streamed", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     ("nbl_sim_set_primary_offset", C.c_int, [C.c_void_p, C.c_uint64]),
     ("nbl_debug_kernel_arch", C.c_int, [C.c_int, C.POINTER(C.c_int32)]),
     ("nbl_debug_philox", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

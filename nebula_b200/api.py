@@ -281,6 +281,17 @@ class Simulation:
         records = np.ascontiguousarray(records, PRI_DTYPE)
         check(lib().nbl_sim_push_primaries(self._h, records.ctypes.data, len(records)))
 
+    def push_streamed(self, records):
+        """Queue primaries from page-locked host memory (a PRI_DTYPE array,
+        e.g. a view of a pinned torch tensor) without waiting for the copy:
+        the next run admits them as their chunks land.  The array must stay
+        unchanged until the run returns; it is kept referenced until then."""
+        records = np.asarray(records, PRI_DTYPE)
+        if not records.flags.c_contiguous:
+            raise ValueError("streamed primaries must be one contiguous array")
+        check(lib().nbl_sim_push_primaries_streamed(self._h, records.ctypes.data, len(records)))
+        self._streamed = getattr(self, "_streamed", []) + [records]
+
     def push_device(self, ptr, n):
         check(lib().nbl_sim_push_primaries_device(self._h, C.c_void_p(ptr), n))
 
@@ -408,6 +419,7 @@ class Simulation:
 
     def reset(self):
         check(lib().nbl_sim_reset(self._h))
+        self._streamed = []
 
     def close(self):
         if getattr(self, "_h", None):

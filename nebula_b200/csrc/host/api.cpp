@@ -101,6 +101,14 @@ struct nbl_sim {
 	bool sink_registered = false;           // page-locked by this library
 	uint32_t dev_det_cap = 0;               // capacity of the device record buffer
 	cudaStream_t cstream = nullptr;         // the copies into the sink
+	// Streamed pushes: primaries copied from page-locked host memory in
+	// chunks on the copy stream; after each chunk the count of primaries in
+	// device memory is copied to `avail`, and the refill admits only those.
+	DevBuf avail;                           // one word: primaries in device memory
+	uint32_t* avail_host = nullptr;         // page-locked counts, one per chunk in flight
+	static constexpr int AVAIL_SLOTS = 64;
+	cudaEvent_t ev_first = nullptr;         // the first chunk of a streamed push has landed
+	bool stream_pending = false;            // a streamed push may still be copying
 	uint64_t sink_fill = 0;                 // records copied (or on their way) into the sink
 	uint32_t dev_copied = 0;                // of the device buffer, records already sent to the sink
 	bool sink_overflow = false;             // a run had more records than the sink holds
@@ -136,7 +144,10 @@ struct nbl_sim {
 	~nbl_sim()
 	{
 		release_sink();
+		if (cstream) cudaStreamSynchronize(cstream);
 		if (cstream) cudaStreamDestroy(cstream);
+		if (avail_host) cudaFreeHost(avail_host);
+		if (ev_first) cudaEventDestroy(ev_first);
 		if (graph) cudaGraphExecDestroy(graph);
 		if (ev0) cudaEventDestroy(ev0);
 		if (ev1) cudaEventDestroy(ev1);
@@ -270,7 +281,12 @@ struct nbl_sim {
 			// every iteration with work makes flights; none for two whole
 			// graphs means the run cannot progress: report it, never spin
 			const uint64_t progress = flights_done();
-			if (progress == last_progress) {
+			if (progress == last_progress && stream_pending) {
+				// nothing to do until more primaries land: wait for the copies
+				CU(cudaStreamSynchronize(cstream));
+				stream_pending = false;
+				stalled = 0;
+			} else if (progress == last_progress) {
 				if (++stalled >= 2)
 					throw Error(NBL_ERR_POOL_OVERFLOW, "no electron moved for two graphs of iterations");
 			} else {
@@ -336,6 +352,8 @@ struct nbl_sim {
 
 	void reset_device_state()
 	{
+		if (cstream)
+			CU(cudaStreamSynchronize(cstream));   // no copy may still land in the buffers
 		CU(cudaMemsetAsync(ctrl.p, 0, ctrl.bytes, stream));
 		CU(cudaMemsetAsync(counters.p, 0, counters.bytes, stream));
 		CU(cudaMemsetAsync(n_detected.p, 0, n_detected.bytes, stream));
@@ -358,6 +376,8 @@ struct nbl_sim {
 		sink_fill = 0;
 		dev_copied = 0;
 		sink_overflow = false;
+		sp.n_avail = nullptr;
+		stream_pending = false;
 	}
 
 	void ensure_primary_capacity(uint64_t need)
@@ -874,11 +894,15 @@ static void push_common(nbl_sim* s, const void* src, int64_t n, cudaMemcpyKind k
 		"primary offset + primaries must stay below 2^32");
 	if (n == 0) return;
 	set_device(s->device);
+	if (s->cstream)
+		CU(cudaStreamSynchronize(s->cstream));    // a streamed push before this one has landed
 	s->ensure_primary_capacity(s->n_pri + n);
 	CU(cudaMemcpyAsync(s->primaries.as<Record36>() + s->n_pri, src, (size_t)n * sizeof(Record36), kind, s->stream));
 	CU(cudaStreamSynchronize(s->stream));
 	s->n_pri += n;
 	s->sp.n_primaries = (uint32_t)s->n_pri;
+	s->sp.n_avail = nullptr;                      // every pushed primary is in device memory
+	s->stream_pending = false;
 	s->graph_dirty = true;
 }
 
@@ -887,6 +911,59 @@ nbl_status nbl_sim_push_primaries(nbl_sim* s, const nbl_record* recs, int64_t n)
 	return guard([&] {
 		require(recs != nullptr || n == 0, "null records");
 		push_common(s, recs, n, cudaMemcpyHostToDevice);
+	});
+}
+
+nbl_status nbl_sim_push_primaries_streamed(nbl_sim* s, const nbl_record* recs, int64_t n)
+{
+	return guard([&] {
+		require(s != nullptr, "null simulation");
+		require(recs != nullptr || n == 0, "null records");
+		require(n >= 0, "negative count");
+		require(s->n_pri + (uint64_t)n < 0xFFFFFFFFull, "at most 2^32-1 primaries per simulation");
+		require(s->sp.tag_base + s->n_pri + (uint64_t)n <= 0xFFFFFFFFull,
+			"primary offset + primaries must stay below 2^32");
+		if (n == 0) return;
+		set_device(s->device);
+		cudaPointerAttributes a{};
+		if (!(cudaPointerGetAttributes(&a, recs) == cudaSuccess && a.type == cudaMemoryTypeHost)) {
+			cudaGetLastError();
+			throw Error(NBL_ERR_INVALID_ARG, "streamed pushes copy from page-locked host memory; "
+				"use nbl_sim_push_primaries for pageable memory");
+		}
+		if (!s->cstream)
+			CU(cudaStreamCreateWithFlags(&s->cstream, cudaStreamNonBlocking));
+		if (!s->avail_host)
+			CU(cudaMallocHost(&s->avail_host, nbl_sim::AVAIL_SLOTS * sizeof(uint32_t)));
+		if (!s->avail.p)
+			s->avail.alloc(sizeof(uint32_t));
+		if (!s->ev_first)
+			CU(cudaEventCreateWithFlags(&s->ev_first, cudaEventDisableTiming));
+		CU(cudaStreamSynchronize(s->cstream));    // earlier copies and their count slots are done
+		s->ensure_primary_capacity(s->n_pri + n);
+		const uint64_t first = s->n_pri;
+		Record36* dst = s->primaries.as<Record36>() + first;
+		// chunks of at least 2^16 primaries, at most AVAIL_SLOTS - 1 of them
+		const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(nbl_sim::AVAIL_SLOTS - 1, n >> 16));
+		const int64_t per = (n + chunks - 1) / chunks;
+		s->avail_host[0] = (uint32_t)first;
+		CU(cudaMemcpyAsync(s->avail.p, s->avail_host, sizeof(uint32_t), cudaMemcpyHostToDevice, s->cstream));
+		int slot = 1;
+		for (int64_t off = 0; off < n; off += per, ++slot) {
+			const int64_t len = std::min(per, n - off);
+			CU(cudaMemcpyAsync(dst + off, recs + off, (size_t)len * sizeof(Record36), cudaMemcpyHostToDevice, s->cstream));
+			s->avail_host[slot] = (uint32_t)(first + off + len);
+			CU(cudaMemcpyAsync(s->avail.p, s->avail_host + slot, sizeof(uint32_t), cudaMemcpyHostToDevice, s->cstream));
+			if (off == 0)
+				CU(cudaEventRecord(s->ev_first, s->cstream));
+		}
+		// the run's first graph starts once the first chunk is in
+		CU(cudaStreamWaitEvent(s->stream, s->ev_first, 0));
+		s->n_pri += n;
+		s->sp.n_primaries = (uint32_t)s->n_pri;
+		s->sp.n_avail = s->avail.as<uint32_t>();
+		s->stream_pending = true;
+		s->graph_dirty = true;
 	});
 }
 

@@ -40,6 +40,7 @@ constexpr int SLOT_SPILL_HEAD = N_QUEUES + 2;
 constexpr int SLOT_SPILL_TAIL = N_QUEUES + 3;
 constexpr int SLOT_SPILL_PUSHED = N_QUEUES + 4;
 constexpr int SLOT_WORK = N_QUEUES + 5;   // items handed out so far in the iteration that reads the slot
+constexpr int SLOT_AVAIL = N_QUEUES + 6;  // primaries in device memory (streamed pushes), as the previous iteration saw
 static_assert(SLOT_WORK < SLOT_WORDS, "control slot too small");
 
 struct Tallies {
@@ -72,6 +73,7 @@ struct StepParams {
 	uint32_t* ctrl;           // 3 slots x SLOT_WORDS
 	const Record36* primaries;
 	uint32_t n_primaries;
+	const uint32_t* n_avail;  // primaries copied so far by a streamed push (null: all n_primaries are there)
 	uint32_t tag_base;        // random-stream tag of primaries[0] (a resumed or sharded scan)
 	Record36* detected;
 	uint32_t* n_detected;

@@ -591,7 +591,10 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 	// while the population is above the refill threshold
 	const bool parked = sp_tail - sp_head > n_drain;
 	const uint32_t room = (e3 < P.refill_below && !parked) ? P.capacity - min(e3, P.capacity) : 0u;
-	const uint32_t left = P.n_primaries - cursor;
+	// a streamed push: only the primaries whose copy had landed when the
+	// previous iteration started (the same snapshot for every thread)
+	const uint32_t avail = P.n_avail ? min(ld_ctrl(cr + SLOT_AVAIL), P.n_primaries) : P.n_primaries;
+	const uint32_t left = avail > cursor ? avail - cursor : 0u;
 	const uint32_t nr = min(min(room, left), P.ramp);
 	const uint32_t total = e3 + nr;
 	// Secondary budget: every item leaves at most one electron in the next
@@ -606,6 +609,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		cw[SLOT_SPILL_HEAD] = sp_head + n_drain;
 		cw[SLOT_SPILL_TAIL] = sp_tail;
 		cw[SLOT_NEW_BUDGET] = se_budget;
+		if (P.n_avail)
+			cw[SLOT_AVAIL] = max(ld_ctrl(P.n_avail), ld_ctrl(cr + SLOT_AVAIL));
 		uint32_t* cz = P.ctrl + zs * SLOT_WORDS;
 #pragma unroll
 		for (int k = 0; k < SLOT_WORDS; ++k)

@@ -263,3 +263,41 @@ def test_loaded_transport_kernel_is_sm100():
     v = C.c_int32()
     _capi.check(_capi.lib().nbl_debug_kernel_arch(0, C.byref(v)))
     assert v.value == 100, v.value
+
+
+def test_streamed_push_equals_a_plain_push(inputs):
+    """Primaries pushed from page-locked memory without waiting for the copy
+    (copied in chunks while the run goes, each admitted once its chunk has
+    landed) give exactly the records of a plain push: alone, after a plain
+    push of the first part, and into a record sink; pageable memory is
+    refused."""
+    import torch
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    pri = primaries.point_beam(200_000, energy=500.0)
+    pri["px"] = np.arange(len(pri)) % 64
+    sim = nb.Simulation(g, [m], capacity=1 << 16, seed=9)
+    sim.push(pri)
+    sim.run()
+    ref = sim.flush_detected()
+    pinned = torch.from_numpy(pri.view(np.uint8).copy()).pin_memory()
+    view = np.frombuffer(pinned.numpy(), dtype=nb.PRI_DTYPE)
+    for split in (0, 70_000):
+        sim.reset()
+        if split:
+            sim.push(pri[:split])
+        sim.push_streamed(view[split:])
+        sim.run()
+        got = sim.flush_detected()
+        assert len(got) == len(ref) and _sorted(got) == _sorted(ref)
+        assert sim.counters()["primaries_started"] == len(pri)
+    sink_mem = torch.empty((len(ref) + 1024) * 36, dtype=torch.uint8).pin_memory()
+    sim.set_record_sink(np.frombuffer(sink_mem.numpy(), dtype=nb.PRI_DTYPE))
+    sim.reset()
+    sim.push_streamed(view)
+    sim.run()
+    assert _sorted(sim.sink_records().copy()) == _sorted(ref)
+    with pytest.raises(nb.NblError) as e:
+        sim.push_streamed(pri.copy())
+    assert e.value.status == 1 and "page-locked" in str(e.value)
+    sim.close()
