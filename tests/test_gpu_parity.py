@@ -61,6 +61,54 @@ def test_ray_query_bit_exact_vs_oracle_many_rays(inputs):
     assert np.array_equal(od[sub].view(np.uint32), o_d.view(np.uint32))
 
 
+def test_ray_query_bit_exact_on_edges_vertices_and_ties(inputs):
+    """Rays aimed at triangle edges and vertices (where u, v or u + v sits on
+    its threshold), rays from cell-aligned points along diagonals (where two
+    or three leaf exits tie) and rays with a zero or tiny direction
+    component: the cases where a comparison cannot be decided from a fast
+    quotient and the IEEE quotient must decide it.  Distance bits and
+    triangle ids equal the oracle's on every ray."""
+    g = nb.Geometry.from_tri_file(inputs["grating.tri"])
+    od_, tr = g.export()
+    inf = g.info()
+    t11 = np.concatenate([np.stack([tr["material_in"], tr["material_out"]], 1).astype(np.float32),
+                          tr["r0"], tr["e1"], tr["e2"]], 1)
+    og = O.Geometry(od_, t11, inf["center"], inf["halfsize"], inf["max_extent"])
+    rng = np.random.default_rng(29)
+    n = 6000
+    ti = rng.integers(0, len(tr), n)
+    r0, e1, e2 = (tr[k][ti].astype(np.float64) for k in ("r0", "e1", "e2"))
+    a = rng.uniform(0, 1, (n, 1))
+    kind = rng.integers(0, 4, n)[:, None]
+    target = np.where(kind == 0, r0 + a * e1,                       # v = 0 edge
+             np.where(kind == 1, r0 + a * e2,                       # u = 0 edge
+             np.where(kind == 2, r0 + a * e1 + (1 - a) * e2,        # u + v = 1 edge
+                      r0 + e1 * (rng.integers(0, 2, (n, 1))))))     # vertices
+    off = rng.standard_normal((n, 3))
+    off /= np.linalg.norm(off, axis=1, keepdims=True)
+    pos = target + off * rng.uniform(0.5, 60.0, (n, 1))
+    d = target - pos
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    # cell-aligned starts along diagonals, and zero / tiny direction components
+    m = 3000
+    gp = np.stack([rng.integers(-140, 140, m), rng.integers(-490, 490, m), rng.integers(-40, 49, m)], 1)
+    gd = rng.choice(np.array([-1.0, 1.0]), (m, 3))
+    gd[: m // 3, rng.integers(0, 3)] = 0.0
+    gd[m // 3: 2 * m // 3, 2] = 1e-39
+    gd /= np.linalg.norm(gd, axis=1, keepdims=True)
+    pos = np.concatenate([pos, gp.astype(np.float64)]).astype(np.float32)
+    d = np.concatenate([d, gd]).astype(np.float32)
+    inside = np.all(np.abs(pos - inf["center"]) < 0.999 * np.asarray(inf["halfsize"]), axis=1)
+    pos, d = pos[inside], d[inside]
+    dist = rng.exponential(80.0, len(pos)).astype(np.float32)
+    im = np.full(len(pos), -123, np.int32)
+    od, ot = g.ray_query(pos, d, dist, None, im)
+    o_d, o_t = og.propagate(pos, d, dist, None, im)
+    assert inside[:n].sum() > n // 2 and (ot >= 0).sum() > n // 4     # the aimed rays do hit
+    assert np.array_equal(ot, o_t)
+    assert np.array_equal(od.view(np.uint32), o_d.view(np.uint32))
+
+
 @pytest.mark.parametrize("which,rank", [("el_imfp", 1), ("el_icdf", 2), ("in_imfp", 1), ("in_omega", 2),
                                         ("in_q", 3), ("in_binding", 3)])
 def test_table_lookup_bit_exact(inputs, which, rank):
