@@ -88,7 +88,13 @@ struct nbl_sim {
 	std::vector<nbl_record> host_records;   // records drained from the device during runs
 	uint32_t records_seen = 0;              // device record count at the last graph boundary
 	uint32_t record_growth = 0;             // most records one graph has added
-	uint32_t* pinned_ctrl = nullptr;
+	uint32_t* pinned_ctrl = nullptr;        // control slot, record count, then the counters
+	static constexpr size_t PINNED_COUNTERS_OFFSET = ((SLOT_WORDS + 4) * sizeof(uint32_t) + 7) & ~(size_t)7;
+	static constexpr size_t PINNED_BYTES = PINNED_COUNTERS_OFFSET + N_COUNTERS * sizeof(unsigned long long);
+	unsigned long long* pinned_counters()
+	{
+		return reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(pinned_ctrl) + PINNED_COUNTERS_OFFSET);
+	}
 
 	// Record sink: page-locked host memory that receives a run's detected
 	// records while it runs.  The kernel appends them to the device buffer;
@@ -194,6 +200,8 @@ struct nbl_sim {
 		CU(cudaMemcpyAsync(pinned_ctrl, ctrl.as<uint32_t>() + slot * SLOT_WORDS, SLOT_WORDS * sizeof(uint32_t),
 			cudaMemcpyDeviceToHost, stream));
 		CU(cudaMemcpyAsync(pinned_ctrl + SLOT_WORDS, n_detected.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+		CU(cudaMemcpyAsync(pinned_counters(), counters.p, N_COUNTERS * sizeof(unsigned long long),
+			cudaMemcpyDeviceToHost, stream));
 		CU(cudaStreamSynchronize(stream));
 		float ms = 0;
 		if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess)
@@ -232,8 +240,19 @@ struct nbl_sim {
 	{
 		uint32_t c[SLOT_WORDS + 1];
 		uint64_t stalled = 0, last_progress = ~0ull;
+		// Records of a finished graph go to the sink once the next graph has
+		// been launched: the copy then runs beside that graph, and the small
+		// reads of the control words (queued behind the graph) never wait
+		// behind a large copy on the copy engine, which would hold back the
+		// next launch for the whole copy.
+		bool sink_pending = false;
+		uint32_t sink_upto = 0;
 		for (uint64_t k = 0; k < max_graphs; ++k) {
 			launch_graph();
+			if (sink_pending) {
+				sink_copy(sink_upto);
+				sink_pending = false;
+			}
 			read_ctrl(c);
 			// records stay on the device until the buffer could not take two
 			// more graphs' worth (the most one graph has added so far, at
@@ -243,15 +262,17 @@ struct nbl_sim {
 			record_growth = std::max(record_growth, ndet >= records_seen ? ndet - records_seen : ndet);
 			const uint64_t reserve = std::max<uint64_t>(2ull * record_growth, sp.det_cap / 4);
 			if (sink) {
-				sink_copy(ndet);
 				if ((uint64_t)ndet + reserve > sp.det_cap) {
 					// the buffer is reused from its start once its records
 					// are in the sink
+					sink_copy(ndet);
 					CU(cudaStreamSynchronize(cstream));
 					CU(cudaMemsetAsync(n_detected.p, 0, sizeof(uint32_t), stream));
 					dev_copied = 0;
 					records_seen = 0;
 				} else {
+					sink_pending = true;
+					sink_upto = ndet;
 					records_seen = ndet;
 				}
 			} else if ((uint64_t)ndet + reserve > sp.det_cap) {
@@ -276,8 +297,11 @@ struct nbl_sim {
 			}
 			const uint64_t active = queued(c) + spill_occupancy(c);
 			const uint64_t left = n_pri - c[SLOT_CURSOR];
-			if (active == 0 && left == 0)
+			if (active == 0 && left == 0) {
+				if (sink_pending)
+					sink_copy(sink_upto);
 				return 0;
+			}
 			// every iteration with work makes flights; none for two whole
 			// graphs means the run cannot progress: report it, never spin
 			const uint64_t progress = flights_done();
@@ -294,6 +318,8 @@ struct nbl_sim {
 			}
 			last_progress = progress;
 		}
+		if (sink_pending)
+			sink_copy(sink_upto);
 		read_ctrl(c);
 		return (int64_t)(queued(c) + spill_occupancy(c) + (n_pri - c[SLOT_CURSOR]));
 	}
@@ -312,12 +338,11 @@ struct nbl_sim {
 		return c[SLOT_SPILL_TAIL] + c[SLOT_SPILL_PUSHED] - c[SLOT_SPILL_HEAD];
 	}
 
-	// flights started plus walks continued: grows in every iteration that has work
+	// flights started plus walks continued (as of the last read_ctrl): grows
+	// in every iteration that has work
 	uint64_t flights_done()
 	{
-		unsigned long long c[N_COUNTERS];
-		CU(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
-		CU(cudaStreamSynchronize(stream));
+		const unsigned long long* c = pinned_counters();
 		return c[CNT_FLIGHTS] + c[CNT_RESUMED];
 	}
 
@@ -725,7 +750,7 @@ nbl_status nbl_sim_create(const nbl_geometry* g, nbl_material* const* materials,
 		}
 		CU(cudaEventCreate(&s->ev0));
 		CU(cudaEventCreate(&s->ev1));
-		CU(cudaMallocHost(&s->pinned_ctrl, (SLOT_WORDS + 4) * sizeof(uint32_t)));
+		CU(cudaMallocHost(&s->pinned_ctrl, nbl_sim::PINNED_BYTES));
 
 		const uint32_t cap = params->capacity ? params->capacity : (1u << 20);
 		require(cap >= 32 && cap <= (1u << 28), "capacity must be 32..2^28");
