@@ -639,10 +639,39 @@ def run_case(args):
              (1.2 M triangles, octree depth <= 12; 300 eV unless given);
     slab:    ``pixels^2 x per_pixel`` primaries on the 1 um Si slab;
     batch:   the 64-job mixed batch with every job's primaries scaled by
-             ``--batch-scale``, in the batched persistent kernel.
-    Small enough for an ncu capture of a few launches on one GPU."""
+             ``--batch-scale``, in the batched persistent kernel;
+    driver:  the drop-in executable (nebula_b200/nebula_b200_gpu) on
+             ``--repeat`` copies of the whole grating scan, its records to a
+             file, as the reference executable is timed (its "Simulation"
+             phase; ``--capacity`` passed on).
+    Small enough for an ncu capture of a few launches on one GPU (driver
+    aside)."""
     import nebula_b200 as nb
     from nebula_b200.synth import workloads, geometry, materials, nmat
+    if args.case == "driver":
+        from nebula_b200 import build
+        with tempfile.TemporaryDirectory() as d:
+            w, tri, mats = make_inputs(d, seed=7)
+            pri_path = os.path.join(d, "scan.pri")
+            raw = np.ascontiguousarray(w.primaries).tobytes()
+            with open(pri_path, "wb") as f:
+                for _ in range(args.repeat):
+                    f.write(raw)
+            out = os.path.join(d, "detected.bin")
+            t0 = time.perf_counter()
+            with open(out, "wb") as sink:
+                r = subprocess.run([build.DRIVER, "--capacity", str(args.capacity), tri, pri_path] + mats,
+                                   stdout=sink, stderr=subprocess.PIPE, text=True, timeout=600)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise RuntimeError(r.stderr[-1000:])
+            phases = dict((k.strip(), float(v)) for k, v in
+                          re.findall(r"([A-Za-z][A-Za-z ]+):\s*([0-9.]+)", r.stderr.split("Timing (seconds):")[-1]))
+            n = args.repeat * len(w.primaries)
+            print(json.dumps({"case": "drop-in executable, %d x the 256x256x100 grating scan" % args.repeat,
+                              "primaries": n, "record_bytes": os.path.getsize(out), "phases_s": phases,
+                              "wall_s": wall, "primaries_per_s": n / phases["Simulation"]}))
+        return
     if args.case == "batch":
         from nebula_b200.tune_mixed_batch import load_mixed_batch
         with tempfile.TemporaryDirectory() as d:
@@ -738,7 +767,7 @@ def main():
     ap.add_argument("--no-rough", action="store_true", help="skip the large-mesh (rough lines) measurement")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own GPU driver beside its CPU driver")
-    ap.add_argument("--case", choices=["grating", "rough", "slab", "batch"],
+    ap.add_argument("--case", choices=["grating", "rough", "slab", "batch", "driver"],
                     help="run one bounded profiling case instead of the benchmark (see run_case)")
     ap.add_argument("--pixels", type=int, default=64, help="--case: pixels per side of the scanned block")
     ap.add_argument("--per-pixel", type=int, default=100, help="--case: primaries per pixel")

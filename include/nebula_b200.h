@@ -93,6 +93,15 @@ nbl_status nbl_load_tri_file(const char* path, nbl_triangle** out, int64_t* n);
 /* Read a .pri file of 36-byte records; release with nbl_free. */
 nbl_status nbl_load_pri_file(const char* path, nbl_record** out, int64_t* n);
 void nbl_free(void* p);
+/* Page-locked host memory for record sinks and streamed pushes: allocate
+ * (release with nbl_host_free), or page-lock memory the caller owns (undo
+ * with nbl_host_unregister before freeing it).  Thin wrappers of the CUDA
+ * runtime's cudaMallocHost / cudaHostRegister, so a host program needs no
+ * CUDA headers; no counterpart in the reference. */
+nbl_status nbl_host_alloc(int64_t bytes, void** out);
+void nbl_host_free(void* p);
+nbl_status nbl_host_register(void* p, int64_t bytes);
+nbl_status nbl_host_unregister(void* p);
 
 /* ------------------------------------------------------------ materials */
 /* A table in the reference's transformed domain (common/util/table_{1,2,3}D):
@@ -287,7 +296,11 @@ nbl_status nbl_sim_push_primaries_streamed(nbl_sim* s, const nbl_record* recs, i
 nbl_status nbl_sim_set_primary_offset(nbl_sim* s, uint64_t first);
 /* Run `iterations` wavefront iterations (rounded up to whole graphs); the
  * number still in flight or queued is returned (gpu_driver::do_iteration,
- * get_running_count). */
+ * get_running_count).  With a record sink, stops early after a graph whose
+ * records the sink could not all take: nbl_sim_sink_count then equals the
+ * sink's capacity, the rest wait in the simulation, and the next
+ * nbl_sim_set_record_sink delivers them first (so a caller can step a run of
+ * any size through two alternating sinks). */
 nbl_status nbl_sim_step(nbl_sim* s, uint32_t iterations, int64_t* running);
 /* Run until every queued primary and its cascade is done. */
 nbl_status nbl_sim_run(nbl_sim* s);
@@ -315,11 +328,14 @@ void nbl_sim_destroy(nbl_sim* s);
  * records each graph of iterations adds to the device buffer are copied into
  * it on a copy stream while the next graph runs, so when nbl_sim_run returns
  * only the last graph's copy has been waited for.  Records of a run start at
- * host[0] after a reset, in the order nbl_sim_drain_detected would return
- * them; a run with more records than `capacity` fails with
- * NBL_ERR_POOL_OVERFLOW.  capacity 0 removes the sink (records stay in the
- * device buffer for nbl_sim_drain_detected again).  No counterpart in the
- * reference (its flush_buffered copies the whole pool per frame). */
+ * host[0] after a reset (or after this call), in the order
+ * nbl_sim_drain_detected would return them; nbl_sim_run with more records
+ * than `capacity` fails with NBL_ERR_POOL_OVERFLOW (nbl_sim_step stops
+ * instead, see there).  Records a stepped run could not fit into the previous
+ * sink go first into this one (with capacity 0, to nbl_sim_drain_detected).
+ * capacity 0 removes the sink (records stay in the device buffer for
+ * nbl_sim_drain_detected again).  No counterpart in the reference (its
+ * flush_buffered copies the whole pool per frame). */
 nbl_status nbl_sim_set_record_sink(nbl_sim* s, nbl_record* host, int64_t capacity);
 /* Records in the sink so far. */
 nbl_status nbl_sim_sink_count(nbl_sim* s, int64_t* n);

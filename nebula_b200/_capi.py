@@ -112,6 +112,10 @@ _DECLS = [
     ("nbl_abi_version", C.c_int, []),
     ("nbl_device_count", C.c_int, [C.POINTER(C.c_int32)]),
     ("nbl_free", None, [C.c_void_p]),
+    ("nbl_host_alloc", C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
+    ("nbl_host_free", None, [C.c_void_p]),
+    ("nbl_host_register", C.c_int, [C.c_void_p, C.c_int64]),
+    ("nbl_host_unregister", C.c_int, [C.c_void_p]),
     ("nbl_load_tri_file", C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Triangle)), i64p]),
     ("nbl_load_pri_file", C.c_int, [C.c_char_p, C.POINTER(C.POINTER(Record)), i64p]),
     ("nbl_material_load", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),

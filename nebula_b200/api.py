@@ -191,6 +191,19 @@ class Material:
             pass
 
 
+def page_lock(array):
+    """Page-lock the memory of a contiguous numpy array in place (for record
+    sinks and streamed pushes without a staging copy); undo with
+    page_unlock before the array is freed."""
+    if not array.flags.c_contiguous or array.nbytes == 0:
+        raise ValueError("page_lock needs a non-empty contiguous array")
+    check(lib().nbl_host_register(array.ctypes.data, array.nbytes))
+
+
+def page_unlock(array):
+    check(lib().nbl_host_unregister(array.ctypes.data))
+
+
 def physics_options(physics=None):
     """``nbl_physics_opts`` from the reference defaults (physics_config.h)
     with the entries of the dict ``physics`` overriding them, e.g.

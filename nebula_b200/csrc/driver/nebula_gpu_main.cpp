@@ -152,12 +152,13 @@ public:
 		cv_.notify_all();
 		thread_.join();
 	}
-	void submit(const std::vector<T>* b, bool* done)
+	void submit(const std::vector<T>* b, bool* done) { submit(b->data(), b->size(), done); }
+	void submit(const T* data, size_t n, bool* done)
 	{
 		std::lock_guard<std::mutex> l(m_);
 		rethrow();
 		*done = false;
-		jobs_.push_back({ b, done });
+		jobs_.push_back({ data, n, done });
 		cv_.notify_all();
 	}
 	// wait until the buffer whose flag this is has been written
@@ -180,7 +181,8 @@ public:
 
 private:
 	struct Job {
-		const std::vector<T>* b;
+		const T* data;
+		size_t n;
 		bool* done;
 	};
 	void rethrow()
@@ -197,7 +199,7 @@ private:
 				return;
 			const Job j = jobs_.front();
 			l.unlock();
-			const bool ok = j.b->empty() || std::fwrite(j.b->data(), sizeof(T), j.b->size(), f_) == j.b->size();
+			const bool ok = j.n == 0 || std::fwrite(j.data, sizeof(T), j.n, f_) == j.n;
 			l.lock();
 			if (!ok)
 				error_ = "writing records failed";
@@ -300,7 +302,7 @@ int run(int argc, char** argv)
 {
 	Cli cli;
 	cli.add("energy-threshold", "0", "Lowest energy to simulate (eV above the vacuum level)");
-	cli.add("capacity", "4194304", "Electrons kept in flight on the GPU");
+	cli.add("capacity", "8388608", "Electrons kept in flight on the GPU");
 	cli.add("prescan-size", "1000", "Accepted for compatibility; no prescan is needed");
 	cli.add("batch-factor", "0.9", "Accepted for compatibility; no input batches are sized");
 	cli.add("seed", "0x78c7e39b", "Random seed");
@@ -310,6 +312,8 @@ int run(int argc, char** argv)
 	cli.add("workers-per-device", "1", "Worker threads (simulation handles) per device");
 	cli.add("chunk", "0", "Primaries a worker takes from the shared queue at a time; 0: a quarter of an even share, "
 		"at least 65536");
+	cli.add("record-buffer", "4194304", "Detected records per page-locked host buffer (two per worker) that receive "
+		"the records while the run goes; 0: drain the device buffer between steps instead");
 	cli.add("first-primary", "0", "Index of the file's first primary within a larger scan (resume, or one process "
 		"per GPU on disjoint files: the records equal one run over the whole scan)");
 	if (kEdep) {
@@ -509,13 +513,39 @@ int run(int argc, char** argv)
 		RecordWriter<nbl_record> writer(detect_f);
 		RecordWriter<nbl_deposit_record> dep_writer(deposit_f ? deposit_f : stdout);
 		std::mutex progress_m;
+		const int64_t record_buffer = (int64_t)cli.u64("record-buffer");
 		auto worker = [&](int w) {
 			nbl_sim* sim = sims[w];
 			std::vector<nbl_record> buf[2];
 			std::vector<nbl_deposit_record> dbuf[2];
 			bool done[2] = { true, true }, ddone[2] = { true, true };
+			// two page-locked record sinks: the run copies its records into one
+			// while the writer writes the other (the device buffer drained
+			// between steps when they cannot be had)
+			nbl_record* sink[2] = { nullptr, nullptr };
+			bool use_sink = record_buffer > 0;
+			for (int k = 0; k < 2 && use_sink; ++k) {
+				void* m = nullptr;
+				if (nbl_host_alloc(record_buffer * (int64_t)sizeof(nbl_record), &m) == NBL_OK)
+					sink[k] = static_cast<nbl_record*>(m);
+				else
+					use_sink = false;
+			}
 			try {
-				int cur = 0;
+				int cur = 0, dcur = 0;
+				if (use_sink)
+					check(nbl_sim_set_record_sink(sim, sink[cur], record_buffer), "record sink");
+				// hand the current sink's records to the writer and continue
+				// into the other one (records that did not fit go there first)
+				auto rotate = [&]() {
+					int64_t n = 0;
+					check(nbl_sim_sink_count(sim, &n), "record count");
+					writer.submit(sink[cur], (size_t)n, &done[cur]);
+					written += n;
+					cur ^= 1;
+					writer.wait(&done[cur]);
+					check(nbl_sim_set_record_sink(sim, sink[cur], record_buffer), "record sink");
+				};
 				auto drain = [&](std::vector<nbl_record>& out) {
 					int64_t pending = 0;
 					check(nbl_sim_detected_count(sim, &pending), "record count");
@@ -555,17 +585,29 @@ int run(int argc, char** argv)
 					check(nbl_sim_set_primary_offset(sim, first_primary + (uint64_t)a), "primary offset");
 					check(nbl_sim_push_primaries(sim, pri + a, n), "pushing primaries");
 					int64_t running = 1, seen = 0;
-					while (running > 0 && !failed) {
+					for (bool full = false; !failed && (running > 0 || full);) {
 						check(nbl_sim_step(sim, 240, &running), "transport");
-						writer.wait(&done[cur]);        // this buffer's previous records are out
-						drain(buf[cur]);
-						writer.submit(&buf[cur], &done[cur]);
-						if (kEdep) {
-							dep_writer.wait(&ddone[cur]);
-							drain_deposits(dbuf[cur]);
-							dep_writer.submit(&dbuf[cur], &ddone[cur]);
+						if (use_sink) {
+							// a step stops early when the sink is full (the records
+							// that did not fit go into the next one); a range's end
+							// hands its records over before the next reset
+							int64_t n = 0;
+							check(nbl_sim_sink_count(sim, &n), "record count");
+							full = n >= record_buffer;
+							if (full || running == 0)
+								rotate();
+						} else {
+							writer.wait(&done[cur]);        // this buffer's previous records are out
+							drain(buf[cur]);
+							writer.submit(&buf[cur], &done[cur]);
+							cur ^= 1;
 						}
-						cur ^= 1;
+						if (kEdep) {
+							dep_writer.wait(&ddone[dcur]);
+							drain_deposits(dbuf[dcur]);
+							dep_writer.submit(&dbuf[dcur], &ddone[dcur]);
+							dcur ^= 1;
+						}
 						nbl_counters c;
 						check(nbl_sim_counters(sim, &c), "counters");
 						started += (int64_t)c.primaries_started - seen;
@@ -587,6 +629,12 @@ int run(int argc, char** argv)
 				if (kEdep)
 					try { dep_writer.wait(&ddone[k]); } catch (const std::exception&) { failed = true; }
 			}
+			// the simulation lets go of the sinks (its copies done) before they are freed
+			if (sink[0] || sink[1]) {
+				nbl_sim_set_record_sink(sim, nullptr, 0);
+				nbl_host_free(sink[0]);
+				nbl_host_free(sink[1]);
+			}
 		};
 		std::vector<std::thread> threads;
 		for (int w = 0; w < n_workers; ++w)
@@ -599,7 +647,6 @@ int run(int argc, char** argv)
 		if (kEdep)
 			dep_writer.finish();
 	}
-	nbl_free(pri);
 	if (detect_f != stdout) std::fclose(detect_f);
 	if (deposit_f && deposit_f != stdout) std::fclose(deposit_f);
 	timer.stop("Simulation");
@@ -610,6 +657,7 @@ int run(int argc, char** argv)
 	timer.print(stderr);
 
 	for (nbl_sim* sim : sims) nbl_sim_destroy(sim);
+	nbl_free(pri);
 	for (nbl_material* m : mats) nbl_material_destroy(m);
 	nbl_geometry_destroy(geom);
 	return 0;

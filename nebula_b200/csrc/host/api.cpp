@@ -118,6 +118,9 @@ struct nbl_sim {
 	uint64_t sink_fill = 0;                 // records copied (or on their way) into the sink
 	uint32_t dev_copied = 0;                // of the device buffer, records already sent to the sink
 	bool sink_overflow = false;             // a run had more records than the sink holds
+	bool sink_full = false;                 // records wait in the device buffer for room in a sink
+	bool timing_pending = false;            // the last graph's events not yet read
+	uint32_t last_ndet = 0;                 // device buffer records as of the last completed graph
 
 	void release_sink()
 	{
@@ -129,7 +132,8 @@ struct nbl_sim {
 	}
 
 	// Send the device buffer's records [dev_copied, ndet) to the sink (they
-	// were written by graphs that have completed).
+	// were written by graphs that have completed).  What the sink has no
+	// room for stays in the device buffer (sink_full) for the next sink.
 	void sink_copy(uint32_t ndet)
 	{
 		ndet = std::min(ndet, sp.det_cap);
@@ -137,14 +141,14 @@ struct nbl_sim {
 			return;
 		uint64_t n = ndet - dev_copied;
 		if (sink_fill + n > (uint64_t)sink_cap) {
-			sink_overflow = true;
+			sink_full = true;
 			n = sink_fill < (uint64_t)sink_cap ? (uint64_t)sink_cap - sink_fill : 0;
 		}
 		if (n)
 			CU(cudaMemcpyAsync(sink + sink_fill, detected.as<nbl_record>() + dev_copied, (size_t)n * sizeof(nbl_record),
 				cudaMemcpyDeviceToHost, cstream));
 		sink_fill += n;
-		dev_copied = ndet;
+		dev_copied += (uint32_t)n;
 	}
 
 	~nbl_sim()
@@ -190,6 +194,7 @@ struct nbl_sim {
 		CU(cudaEventRecord(ev0, stream));
 		CU(cudaGraphLaunch(graph, stream));
 		CU(cudaEventRecord(ev1, stream));
+		timing_pending = true;
 		iteration += graph_iters;
 	}
 
@@ -203,9 +208,11 @@ struct nbl_sim {
 		CU(cudaMemcpyAsync(pinned_counters(), counters.p, N_COUNTERS * sizeof(unsigned long long),
 			cudaMemcpyDeviceToHost, stream));
 		CU(cudaStreamSynchronize(stream));
+		// each graph's device time counted once
 		float ms = 0;
-		if (cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess)
+		if (timing_pending && cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess)
 			kernel_ms += ms;
+		timing_pending = false;
 		std::memcpy(out, pinned_ctrl, SLOT_WORDS * sizeof(uint32_t));
 	}
 
@@ -235,8 +242,11 @@ struct nbl_sim {
 	}
 
 	// Run graphs until done (or `max_graphs` graphs); returns electrons still
-	// in flight plus primaries not yet started.
-	int64_t advance(uint64_t max_graphs)
+	// in flight plus primaries not yet started.  With `stop_when_sink_full`,
+	// stops after the graph whose records the sink could not all take (the
+	// rest wait in the device buffer for the next sink); otherwise records
+	// beyond the sink are dropped and the run reports the overflow.
+	int64_t advance(uint64_t max_graphs, bool stop_when_sink_full = false)
 	{
 		uint32_t c[SLOT_WORDS + 1];
 		uint64_t stalled = 0, last_progress = ~0ull;
@@ -247,6 +257,11 @@ struct nbl_sim {
 		// next launch for the whole copy.
 		bool sink_pending = false;
 		uint32_t sink_upto = 0;
+		if (stop_when_sink_full && sink_full) {
+			// records still wait for a sink: no graph until they have one
+			read_ctrl(c);
+			return (int64_t)(queued(c) + spill_occupancy(c) + (n_pri - c[SLOT_CURSOR]));
+		}
 		for (uint64_t k = 0; k < max_graphs; ++k) {
 			launch_graph();
 			if (sink_pending) {
@@ -259,6 +274,7 @@ struct nbl_sim {
 			// least a quarter of the buffer: a run's early graphs detect less
 			// than its later ones); then they are parked on the host
 			const uint32_t ndet = pinned_ctrl[SLOT_WORDS];
+			last_ndet = ndet;
 			record_growth = std::max(record_growth, ndet >= records_seen ? ndet - records_seen : ndet);
 			const uint64_t reserve = std::max<uint64_t>(2ull * record_growth, sp.det_cap / 4);
 			if (sink) {
@@ -266,9 +282,14 @@ struct nbl_sim {
 					// the buffer is reused from its start once its records
 					// are in the sink
 					sink_copy(ndet);
+					if (sink_full && stop_when_sink_full)
+						return (int64_t)(queued(c) + spill_occupancy(c) + (n_pri - c[SLOT_CURSOR]));
+					if (sink_full)
+						sink_overflow = true;       // the rest is dropped
 					CU(cudaStreamSynchronize(cstream));
 					CU(cudaMemsetAsync(n_detected.p, 0, sizeof(uint32_t), stream));
 					dev_copied = 0;
+					last_ndet = 0;
 					records_seen = 0;
 				} else {
 					sink_pending = true;
@@ -301,6 +322,11 @@ struct nbl_sim {
 				if (sink_pending)
 					sink_copy(sink_upto);
 				return 0;
+			}
+			if (sink_full && stop_when_sink_full) {
+				if (sink_pending)
+					sink_copy(sink_upto);          // nothing more fits; the rest waits
+				return (int64_t)(active + left);
 			}
 			// every iteration with work makes flights; none for two whole
 			// graphs means the run cannot progress: report it, never spin
@@ -401,6 +427,8 @@ struct nbl_sim {
 		sink_fill = 0;
 		dev_copied = 0;
 		sink_overflow = false;
+		sink_full = false;
+		last_ndet = 0;
 		sp.n_avail = nullptr;
 		stream_pending = false;
 	}
@@ -442,6 +470,43 @@ nbl_status nbl_device_count(int32_t* n)
 }
 int nbl_abi_version(void) { return NBL_ABI_VERSION; }
 void nbl_free(void* p) { std::free(p); }
+
+nbl_status nbl_host_alloc(int64_t bytes, void** out)
+{
+	return guard([&] {
+		require(out != nullptr && bytes > 0, "bad page-locked allocation");
+		*out = nullptr;
+		if (cudaMallocHost(out, (size_t)bytes) != cudaSuccess) {
+			cudaGetLastError();
+			*out = nullptr;
+			throw Error(NBL_ERR_OOM, "cannot allocate " + std::to_string(bytes) + " bytes of page-locked host memory");
+		}
+	});
+}
+
+void nbl_host_free(void* p)
+{
+	if (p) cudaFreeHost(p);
+}
+
+nbl_status nbl_host_register(void* p, int64_t bytes)
+{
+	return guard([&] {
+		require(p != nullptr && bytes > 0, "bad host range");
+		if (cudaHostRegister(p, (size_t)bytes, cudaHostRegisterDefault) != cudaSuccess) {
+			cudaGetLastError();
+			throw Error(NBL_ERR_OOM, "cannot page-lock " + std::to_string(bytes) + " bytes of host memory");
+		}
+	});
+}
+
+nbl_status nbl_host_unregister(void* p)
+{
+	return guard([&] {
+		require(p != nullptr, "null pointer");
+		CU(cudaHostUnregister(p));
+	});
+}
 
 nbl_status nbl_load_tri_file(const char* path, nbl_triangle** out, int64_t* n)
 {
@@ -1017,7 +1082,7 @@ nbl_status nbl_sim_step(nbl_sim* s, uint32_t iterations, int64_t* running)
 		require(s != nullptr, "null simulation");
 		set_device(s->device);
 		const uint64_t graphs = (iterations + s->graph_iters - 1) / s->graph_iters;
-		const int64_t r = s->advance(std::max<uint64_t>(graphs, 1));
+		const int64_t r = s->advance(std::max<uint64_t>(graphs, 1), true);
 		s->sink_wait();
 		if (running) *running = r;
 		s->check_errors();
@@ -1039,6 +1104,8 @@ nbl_status nbl_sim_run(nbl_sim* s)
 		const uint64_t max_graphs = bound / s->graph_iters + 2;
 		const int64_t left = s->advance(max_graphs);
 		s->sink_wait();
+		if (s->sink_full)
+			s->sink_overflow = true;
 		s->check_errors();
 		if (left != 0)
 			throw Error(NBL_ERR_BUDGET_EXCEEDED, "run did not finish within its iteration bound");
@@ -1052,6 +1119,10 @@ nbl_status nbl_sim_set_record_sink(nbl_sim* s, nbl_record* host, int64_t capacit
 		require(capacity >= 0 && capacity <= 0xFFFFFFFFll && (host || capacity == 0), "bad record sink");
 		set_device(s->device);
 		CU(cudaStreamSynchronize(s->stream));
+		// records a stepped run could not fit into the previous sink wait in
+		// the device buffer after the ones it took: they go first into the new
+		// sink (or, with no new sink, to the host store)
+		const bool carry = s->sink && s->dev_copied < s->last_ndet;
 		s->release_sink();
 		if (capacity > 0) {
 			cudaPointerAttributes a{};
@@ -1069,13 +1140,26 @@ nbl_status nbl_sim_set_record_sink(nbl_sim* s, nbl_record* host, int64_t capacit
 			s->sink = host;
 			s->sink_cap = capacity;
 		}
+		s->sink_fill = 0;
+		s->sink_overflow = false;
+		s->sink_full = false;
+		if (carry && s->sink) {
+			s->sink_copy(s->last_ndet);
+			CU(cudaStreamSynchronize(s->cstream));
+			return;
+		}
+		if (carry) {
+			const uint32_t n = s->last_ndet - s->dev_copied;
+			const size_t old = s->host_records.size();
+			s->host_records.resize(old + n);
+			CU(cudaMemcpyAsync(s->host_records.data() + old, s->detected.as<nbl_record>() + s->dev_copied,
+				(size_t)n * sizeof(nbl_record), cudaMemcpyDeviceToHost, s->stream));
+		}
 		// records of later runs go to the device buffer either way
 		s->sp.detected = s->detected.as<Record36>();
 		s->sp.det_cap = s->dev_det_cap;
-		s->sink_fill = 0;
 		s->dev_copied = 0;
-		s->sink_overflow = false;
-		s->graph_dirty = true;
+		s->last_ndet = 0;
 		CU(cudaMemsetAsync(s->n_detected.p, 0, sizeof(uint32_t), s->stream));
 		CU(cudaStreamSynchronize(s->stream));
 		s->records_seen = 0;

@@ -81,19 +81,25 @@ def test_not_enough_materials(driver, tmp_path):
 @pytest.mark.gpu
 @pytest.mark.skipif(not has_gpu(), reason="needs a CUDA device")
 def test_records_equal_the_api_run(driver, slab_files):
+    """The default page-locked record buffers; buffers of 3 000 records over
+    ranges of 20 000 primaries (steps stop on a full buffer, records that did
+    not fit carried into the next one, several times within a graph); and
+    the device buffer drained between steps: the same records each time."""
     tri, pri, mat, p = slab_files
-    r = _run([driver, "--seed", "4242", "--capacity", "65536", tri, pri, mat])
-    assert r.returncode == 0, r.stderr[-2000:]
-    assert b"Simulation successful" in r.stderr and b"Timing (seconds):" in r.stderr
-    got = np.frombuffer(r.stdout, dtype=nb.PRI_DTYPE)
     sim = nb.Simulation(nb.Geometry.from_tri_file(tri), [nb.Material.load(mat)], capacity=1 << 20, seed=4242)
     sim.push(p)
     sim.run()
     ref = sim.flush_detected()
     sim.close()
     key = lambda a: np.sort(a.view(np.dtype((np.void, 36))).ravel()).tobytes()
-    assert len(got) == len(ref) > 0.5 * len(p)
-    assert key(got) == key(ref)
+    for extra in ([], ["--record-buffer", "3000", "--chunk", "20000"], ["--record-buffer", "0"]):
+        r = _run([driver, "--seed", "4242", "--capacity", "65536"] + extra + [tri, pri, mat])
+        assert r.returncode == 0, r.stderr[-2000:]
+        assert b"Simulation successful" in r.stderr and b"Timing (seconds):" in r.stderr
+        got = np.frombuffer(r.stdout, dtype=nb.PRI_DTYPE)
+        assert len(got) == len(ref) > 0.5 * len(p), extra
+        assert key(got) == key(ref), extra
+        assert ("%d detected electrons written" % len(ref)).encode() in r.stderr
 
 
 @pytest.mark.gpu

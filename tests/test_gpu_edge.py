@@ -300,4 +300,58 @@ def test_streamed_push_equals_a_plain_push(inputs):
     with pytest.raises(nb.NblError) as e:
         sim.push_streamed(pri.copy())
     assert e.value.status == 1 and "page-locked" in str(e.value)
+    # a plain array page-locked in place streams the same way
+    plain = pri.copy()
+    nb.page_lock(plain)
+    sim.set_record_sink(None)
+    sim.reset()
+    sim.push_streamed(plain)
+    sim.run()
+    assert _sorted(sim.flush_detected()) == _sorted(ref)
+    nb.page_unlock(plain)
+    sim.close()
+
+
+def test_stepped_run_through_two_alternating_small_sinks(inputs):
+    """A stepped run whose records far outgrow the sink: each step stops when
+    the sink is full, the records that did not fit wait and go first into
+    the next sink, and the sinks taken in turn hold exactly the records of a
+    plain run.  nbl_sim_run with the same small sink still reports the
+    overflow."""
+    import torch
+    from nebula_b200.synth import primaries
+    g, m = _slab(inputs)
+    pri = primaries.point_beam(60_000, energy=800.0)
+    sim = nb.Simulation(g, [m], capacity=1 << 15, seed=21)
+    sim.push(pri)
+    sim.run()
+    ref = sim.flush_detected()
+    cap = len(ref) // 9
+    mem = [torch.empty(cap * 36, dtype=torch.uint8).pin_memory() for _ in range(2)]
+    sinks = [np.frombuffer(x.numpy(), dtype=nb.PRI_DTYPE) for x in mem]
+    sim.reset()
+    cur = 0
+    sim.set_record_sink(sinks[cur])
+    sim.push(pri)
+    parts, full_stops = [], 0
+    while True:
+        running = sim.do_iteration(24)
+        n = len(sim.sink_records())
+        if n == cap:
+            full_stops += 1
+            parts.append(sim.sink_records().copy())
+            cur ^= 1
+            sim.set_record_sink(sinks[cur])
+            continue
+        if running == 0:
+            parts.append(sim.sink_records().copy())
+            break
+    got = np.concatenate(parts)
+    assert full_stops >= 8
+    assert len(got) == len(ref) and _sorted(got) == _sorted(ref)
+    sim.reset()
+    sim.push(pri)
+    with pytest.raises(nb.NblError) as e:
+        sim.run()
+    assert e.value.status == 6
     sim.close()
