@@ -55,6 +55,7 @@ def test_usage_and_bad_arguments(driver, slab_files):
     tri, pri, mat, _ = slab_files
     r = _run([driver])
     assert r.returncode == 1 and r.stdout == b"" and b"Usage: nebula_b200_gpu" in r.stderr
+    assert b"--record-buffer" in r.stderr and b"--workers-per-device" in r.stderr
     r = _run([driver, "--no-such-option", "1", tri, pri, mat])
     assert r.returncode == 1 and b"unknown option --no-such-option" in r.stderr
     # the slab needs material 0: none given
