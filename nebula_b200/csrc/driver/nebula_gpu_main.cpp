@@ -76,7 +76,8 @@ struct Cli {
 
 	void add(const char* key, const char* def, const char* help) { opts[key] = { def, help }; }
 
-	// --key=value, --key value (gpu_main.cu's cli_params forms)
+	// --key=value, --key value, --key = value (the forms gpu_main.cu's
+	// cli_params accepts, common/cli_params.h:55-90)
 	void parse(int argc, char** argv)
 	{
 		for (int i = 1; i < argc; ++i) {
@@ -89,6 +90,8 @@ struct Cli {
 					key = key.substr(0, eq);
 				} else if (i + 1 < argc) {
 					value = argv[++i];
+					if (value == "=" && i + 1 < argc)
+						value = argv[++i];
 				}
 				auto it = opts.find(key);
 				if (it == opts.end())

@@ -64,6 +64,9 @@ def test_usage_and_bad_arguments(driver, slab_files):
     # the physics banner reports the selection (before any device call)
     r = _run([driver, "--inelastic-model", "1", "--interface-absorption", "1", tri, pri, mat])
     assert b"inelastic: kieft_inelastic" in r.stderr and b"interface absorption 1" in r.stderr
+    # the reference parser's other forms: --key=value and --key = value
+    r = _run([driver, "--inelastic-model=1", "--interface-absorption", "=", "1", tri, pri, mat])
+    assert b"inelastic: kieft_inelastic" in r.stderr and b"interface absorption 1" in r.stderr
 
 
 def test_not_enough_materials(driver, tmp_path):
