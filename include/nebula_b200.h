@@ -416,10 +416,12 @@ typedef struct nbl_batch_params {
 void nbl_batch_params_defaults(nbl_batch_params* p);
 
 typedef struct nbl_batch nbl_batch;
+/* 1..64 geometries (staged in each block's shared memory), 1..127 materials. */
 nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geometries,
 	nbl_material* const* materials, int32_t n_materials, const nbl_batch_params* params, nbl_batch** out);
-/* Jobs and the batch's primary array (host records, copied; each job's range
- * [first, first+count) must lie inside it, ranges in increasing order). */
+/* 1..255 jobs and the batch's primary array (host records, copied; each
+ * job's range [first, first+count) must lie inside it, ranges in increasing
+ * order). */
 nbl_status nbl_batch_set_jobs(nbl_batch* b, const nbl_batch_job* jobs, int32_t n_jobs, const nbl_record* primaries,
 	int64_t n_primaries);
 /* Run every job to completion in one persistent launch. */

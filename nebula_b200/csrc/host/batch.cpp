@@ -123,6 +123,8 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 	return guard([&] {
 		require(geometries && materials && params && out, "null argument");
 		require(n_geometries >= 1 && n_materials >= 1 && n_materials <= 127, "bad counts");
+		require(n_geometries <= NBL_BATCH_MAX_GEOMS, "at most " + std::to_string(NBL_BATCH_MAX_GEOMS) +
+			" geometries per batch");
 		for (int i = 0; i < n_geometries; ++i) {
 			require(geometries[i] != nullptr, "null geometry");
 			for (const nbl_triangle& t : geometries[i]->g.tris)
@@ -230,6 +232,7 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 		b->words.alloc(4 * sizeof(uint32_t));   // barrier count, generation, error, iterations
 		BatchParams& bp = b->bp;
 		bp.geoms = b->geom_views.as<DevGeometry>();
+		bp.n_geoms = (int32_t)b->geoms.size();
 		bp.bar_count = b->words.as<uint32_t>();
 		bp.bar_gen = bp.bar_count + 1;
 		bp.err = bp.bar_count + 2;

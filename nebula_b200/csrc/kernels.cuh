@@ -117,9 +117,14 @@ struct DevJob {
 };
 
 // Per-job state of a batched (persistent) run.
+// A batch's geometry and job tables are staged in each block's shared memory.
+constexpr int NBL_BATCH_MAX_GEOMS = 64;
+constexpr int NBL_BATCH_MAX_JOBS = 255;
+
 struct BatchParams {
 	const DevGeometry* geoms;
 	const DevJob* jobs;
+	int32_t n_geoms;
 	int32_t n_jobs;
 	unsigned long long* job_se;     // detected with E < 50 eV, per job
 	unsigned long long* job_bse;    // detected with E >= 50 eV, per job

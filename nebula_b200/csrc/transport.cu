@@ -425,13 +425,13 @@ __device__ __forceinline__ void store_electron(const Queue& q, uint32_t slot, co
 __device__ __forceinline__ uint32_t ld_ctrl(const uint32_t* p) { return __ldcg(p); }
 
 // Job of a batched primary (global index g): the last job whose first
-// primary is <= g.
-__device__ __forceinline__ uint32_t job_of(const BatchParams& B, uint32_t g)
+// primary is <= g (`jobs`: the block's shared copy of the job table).
+__device__ __forceinline__ uint32_t job_of(const DevJob* jobs, int n_jobs, uint32_t g)
 {
-	int lo = 0, hi = B.n_jobs - 1;
+	int lo = 0, hi = n_jobs - 1;
 	while (lo < hi) {
 		const int mid = (lo + hi + 1) >> 1;
-		if (__ldg(&B.jobs[mid].first) <= g) lo = mid; else hi = mid - 1;
+		if (jobs[mid].first <= g) lo = mid; else hi = mid - 1;
 	}
 	return (uint32_t)lo;
 }
@@ -563,7 +563,7 @@ __device__ __forceinline__ void deposit(const StepParams& P, bool scat, const El
 
 template<bool ADJ, bool BATCH, bool DEP = false, uint32_t PHC = 0u>
 __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchParams& B, uint32_t it, LocalCounters& lc,
-	float* s_lane = nullptr)
+	float* s_lane = nullptr, const DevGeometry* s_geoms = nullptr, const DevJob* s_jobs = nullptr)
 {
 	// physics selection bits: a compile-time constant in the instantiations
 	// for the default selection (its option tests fold away, and the code of
@@ -676,8 +676,8 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 			p.dir = v3(ld_stream(&r->dx), ld_stream(&r->dy), ld_stream(&r->dz));
 			p.E = ld_stream(&r->E);
 			if (BATCH) {
-				const uint32_t j = job_of(B, qi);
-				tag = (j << 24) | (qi - __ldg(&B.jobs[j].first));
+				const uint32_t j = job_of(s_jobs, B.n_jobs, qi);
+				tag = (j << 24) | (qi - s_jobs[j].first);
 			} else {
 				tag = P.tag_base + qi;
 			}
@@ -691,11 +691,10 @@ __device__ __forceinline__ bool step_iteration(const StepParams& P, const BatchP
 		if (BATCH) {
 			job = tag >> 24;
 			stream_tag = tag & 0xFFFFFFu;
-			const DevJob* J = B.jobs + (kind >= 0 ? job : 0u);
-			rv.geom = B.geoms + __ldg(&J->geom);
-			rv.key.k0 = __ldg(&J->key.k0);
-			rv.key.k1 = __ldg(&J->key.k1);
-			rec_index = __ldg(&J->first) + stream_tag;
+			const DevJob& J = s_jobs[kind >= 0 ? job : 0u];
+			rv.geom = s_geoms + J.geom;
+			rv.key = J.key;
+			rec_index = J.first + stream_tag;
 		} else {
 			rv.geom = &P.geom;
 			rv.key = P.key;
@@ -917,13 +916,22 @@ __global__ void __launch_bounds__(512, 2) k_batch(const __grid_constant__ StepPa
 	const __grid_constant__ BatchParams B)
 {
 	__shared__ uint32_t s_counters[N_COUNTERS];
+	// the geometry and job tables every item looks up, staged in shared
+	// memory for the whole launch: the walk reads the geometry's fields on
+	// its chain of dependent loads, and shared loads are the shorter ones
+	__shared__ DevGeometry s_geoms[NBL_BATCH_MAX_GEOMS];
+	__shared__ DevJob s_jobs[NBL_BATCH_MAX_JOBS];
 	for (int k = threadIdx.x; k < N_COUNTERS; k += blockDim.x)
 		s_counters[k] = 0u;
+	for (int k = threadIdx.x; k < B.n_geoms; k += blockDim.x)
+		s_geoms[k] = B.geoms[k];
+	for (int k = threadIdx.x; k < B.n_jobs; k += blockDim.x)
+		s_jobs[k] = B.jobs[k];
 	__syncthreads();
 	LocalCounters lc{ s_counters };
 	uint32_t it = 0;
 	for (; it < B.max_iterations; ++it) {
-		if (!step_iteration<ADJ, true, false, PHC>(P, B, it, lc))
+		if (!step_iteration<ADJ, true, false, PHC>(P, B, it, lc, nullptr, s_geoms, s_jobs))
 			break;
 		if (!grid_barrier(B))
 			break;
