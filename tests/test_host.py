@@ -186,6 +186,16 @@ def test_material_count_checked(inputs):
     assert e.value.status == 1
 
 
+def test_batch_limits_checked_before_any_device_work(inputs):
+    """A batch takes at most 64 geometries (its geometry table lives in each
+    block's shared memory): more are an argument error, on any machine."""
+    g = nb.Geometry.from_tri_file(inputs["slab.tri"])
+    m = nb.Material.load(inputs["si.nmat"])
+    with pytest.raises(nb.NblError) as e:
+        nb.Batch([g] * 65, [m], capacity=1024)
+    assert e.value.status == 1 and "64 geometries" in str(e.value)
+
+
 def test_octree_builder_rough_lines_matches_reference(tmp_path):
     """Line-edge-roughness grating (the large-mesh geometry at reduced
     length: 4 lines, 40 nm long, ~25 k triangles): the multithreaded top-down
