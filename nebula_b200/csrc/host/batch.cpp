@@ -149,8 +149,6 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 		require(thr <= 1.0f, "refill_threshold must be in (0, 1]");
 		b->block = params->block_size ? (int)params->block_size : 256;
 		require(b->block == 128 || b->block == 256 || b->block == 512, "block_size must be 128, 256 or 512");
-		b->grid = batch_grid_size(b->device, b->block);
-		require(b->grid > 0, "the batched kernel does not fit on this device with that block size");
 
 		std::vector<DevGeometry> views;
 		for (int i = 0; i < n_geometries; ++i) {
@@ -171,6 +169,9 @@ nbl_status nbl_batch_create(const nbl_geometry* const* geometries, int32_t n_geo
 		StepParams& sp = b->sp;
 		sp.mats = b->mats.mats.as<DevMaterial>();
 		sp.n_mat = n_materials;
+		// co-resident grid with the staged materials' shared memory
+		b->grid = batch_grid_size(b->device, b->block, sp);
+		require(b->grid > 0, "the batched kernel does not fit on this device with that block size");
 		sp.energy_threshold = params->energy_threshold;
 		sp.capacity = cap;
 		sp.qcap = factor * cap;

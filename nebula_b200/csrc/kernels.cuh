@@ -151,6 +151,6 @@ int step_grid_size(int device, int block, const StepParams& p);
 // binary architecture (major * 10 + minor) of the loaded transport kernel
 cudaError_t step_binary_version(int device, int* version);
 cudaError_t launch_batch(const StepParams& p, const BatchParams& b, int grid, int block, cudaStream_t s);
-int batch_grid_size(int device, int block);
+int batch_grid_size(int device, int block, const StepParams& p);
 
 }  // namespace nbl

@@ -136,3 +136,26 @@ def test_batch_record_overflow_is_an_error(small_batch):
         b.run()
     assert e.value.status == 6 and "record_capacity" in str(e.value)
     b.close()
+
+
+def test_the_largest_material_table_gives_the_same_records(small_batch):
+    """127 materials (the most a simulation takes; the jobs use the first two):
+    the batched kernel stages every material's descriptor in shared memory
+    (40.6 KB per block, above its default 48 KB limit together with its
+    geometry and job tables), and the records equal those with two
+    materials, batched and plain."""
+    geoms, mats, jobs = small_batch
+    many = list(mats) + [mats[1]] * (127 - len(mats))
+    ref = _plain_records(geoms, mats, jobs)
+    b = nb.Batch(geoms, many, capacity=1 << 14, block_size=512, record_capacity=1 << 20)
+    b.set_jobs(jobs)
+    b.run()
+    for k, (got, want) in enumerate(zip(b.job_records(), ref)):
+        assert _sorted(got) == _sorted(want), k
+    b.close()
+    gi, seed, pri = jobs[-1]
+    sim = nb.Simulation(geoms[gi], many, capacity=1 << 14, seed=seed)
+    sim.push(pri)
+    sim.run()
+    assert _sorted(sim.flush_detected()) == _sorted(ref[-1])
+    sim.close()
