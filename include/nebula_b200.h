@@ -95,9 +95,10 @@ nbl_status nbl_load_pri_file(const char* path, nbl_record** out, int64_t* n);
 void nbl_free(void* p);
 /* Page-locked host memory for record sinks and streamed pushes: allocate
  * (release with nbl_host_free), or page-lock memory the caller owns (undo
- * with nbl_host_unregister before freeing it).  Thin wrappers of the CUDA
- * runtime's cudaMallocHost / cudaHostRegister, so a host program needs no
- * CUDA headers; no counterpart in the reference. */
+ * with nbl_host_unregister before freeing it; a range already page-locked
+ * is NBL_ERR_INVALID_ARG).  Thin wrappers of the CUDA runtime's
+ * cudaMallocHost / cudaHostRegister, so a host program needs no CUDA
+ * headers; no counterpart in the reference. */
 nbl_status nbl_host_alloc(int64_t bytes, void** out);
 void nbl_host_free(void* p);
 nbl_status nbl_host_register(void* p, int64_t bytes);

@@ -493,8 +493,11 @@ nbl_status nbl_host_register(void* p, int64_t bytes)
 {
 	return guard([&] {
 		require(p != nullptr && bytes > 0, "bad host range");
-		if (cudaHostRegister(p, (size_t)bytes, cudaHostRegisterDefault) != cudaSuccess) {
+		const cudaError_t e = cudaHostRegister(p, (size_t)bytes, cudaHostRegisterDefault);
+		if (e != cudaSuccess) {
 			cudaGetLastError();
+			if (e == cudaErrorHostMemoryAlreadyRegistered)
+				throw Error(NBL_ERR_INVALID_ARG, "the host range is already page-locked");
 			throw Error(NBL_ERR_OOM, "cannot page-lock " + std::to_string(bytes) + " bytes of host memory");
 		}
 	});

@@ -303,6 +303,9 @@ def test_streamed_push_equals_a_plain_push(inputs):
     # a plain array page-locked in place streams the same way
     plain = pri.copy()
     nb.page_lock(plain)
+    with pytest.raises(nb.NblError) as e:
+        nb.page_lock(plain)
+    assert e.value.status == 1 and "already page-locked" in str(e.value)
     sim.set_record_sink(None)
     sim.reset()
     sim.push_streamed(plain)
