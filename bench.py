@@ -25,7 +25,8 @@ mesh (``rough_lines``); the reference CPU driver on a bounded sample
 SM clocks sampled during the timed region (``clocks``).
 
 Multi-GPU (torchrun): replicas, one scan per rank with its own seed (weak
-scaling); time = max over ranks.  --impl reference times the reference's own
+scaling); time = max over ranks.  The single-GPU measurements (batched,
+adjoint, rough lines, CPU baseline) are on the one-GPU line only.  --impl reference times the reference's own
 multithreaded CPU driver (oracle/_ref/nebula_cpu_mt built from its sources)
 on a bounded sample of the same scan with all host threads; its line also
 carries the reference's own GPU driver (oracle/_ref/nebula_gpu, gpu_main.cu
@@ -927,11 +928,13 @@ def main():
             "clocks": clocks,
         }
         sim.close()
-        if not args.no_batch:
+        # the single-GPU measurements ride on the one-GPU line only (every
+        # rank skips them alike, so the ranks' collective steps stay equal)
+        if not args.no_batch and world == 1:
             out["batched"] = batched_vs_plain(args, dev, d)
-        if not args.no_adjoint:
+        if not args.no_adjoint and world == 1:
             out["adjoint"] = adjoint_vs_forward(args, dev, d)
-        if not args.no_rough:
+        if not args.no_rough and world == 1:
             out["rough_lines"] = rough_lines(args, dev, d)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             try:
